@@ -1,0 +1,327 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 key-walk search: keys/s on the plain GPU search.
+
+Workload (the plain GPU search): one 8-hex-digit prefix drawn from the seed,
+aspect lxmf.delivery, every lane starting from its own seeded clamped X25519
+scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, B = 64 keys
+per inversion, 2^36 keys walked in total over the timed steps (a step is one
+launch that walks every lane `iters` batches further).  Synthetic, seeded
+inputs; no dataset is involved.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is device-timed (CUDA events on the
+launching stream, max over ranks), `e2e` goes through the C ABI's
+synchronous lxmfv_launch with host buffers, `cpu_baseline` is the restated
+CPU search on this host's cores, `roofline` relates the walk kernel's
+multiply work to the measured IMAD rate of this GPU.
+With --impl reference, the reference's own kernel body (src/gpu/common.h,
+built for the host) is timed on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "lxmf-vanity_b200"))
+
+TOTAL_KEYS = 1 << 36
+BATCH = 64
+SEED = 3
+METRIC = "keys/s, plain GPU search (8-hex prefix, 2^36 keys, B=64), bit-exact"
+
+
+def wide_products_per_key(b: int) -> float:
+    """32x32->64 products per key with 8 x 32-bit limbs: a field multiply is
+    64 + 8 (fold by 38), a square 36 + 8; per key (8 + 11/B) M + (2 + 254/B) S."""
+    return (8 + 11 / b) * 72 + (2 + 254 / b) * 44
+
+
+def parse() -> argparse.Namespace:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--lanes", type=int, default=0, help="walker lanes per GPU (0: two full waves)")
+    p.add_argument("--batch", type=int, default=BATCH)
+    p.add_argument("--block", type=int, default=0)
+    p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "out", "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_port(prefix: str, seconds: float = 2.5) -> dict:
+    """The restated CPU search (KeyWalk + search of src/main.rs, B = 256,
+    5 x 51-bit field) on every host core, for a bounded sample."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    pfx = O.prefix_parse(prefix)
+    rate, keys, _ = O.bench_search(threads, 1 << 14, SEED, pfx)  # calibration
+    per_thread = max(1 << 14, int(rate * seconds / threads))
+    rate, keys, _ = O.bench_search(threads, per_thread, SEED, pfx)
+    return {"value": rate, "unit": "keys/s", "cores": threads, "kind": "port",
+            "sample": f"{keys} keys: {threads} threads x {per_thread} keys each from seeded starts, "
+                      f"prefix {prefix}, restated KeyWalk (B=256) + double SHA-256 per key"}
+
+
+def reference_cpu(prefix: str, steps: int, warmup: int, step_seconds: float = 2.0) -> dict:
+    """The reference's own kernel body (common.h walk_thread, B = 64) built for
+    the host, on every host core.  Each step walks a bounded sample."""
+    import ctypes as C
+
+    import numpy as np
+
+    from oracle import oracle as O
+    r = O.ref()
+    workers = os.cpu_count() or 1
+    if r is None:
+        port = cpu_baseline_port(prefix, step_seconds)
+        return dict(port, steps=0)
+    lanes = workers * 4
+    ident = O.seeded_identity(SEED)
+    k0, ed_seed, off = ident
+    scal, _ = O.seeded_scalars(SEED, off, lanes - 1)
+    starts = [k0] + [bytes(s) for s in scal]
+    upc = np.zeros((lanes, 16), np.uint32)
+    for t, k in enumerate(starts):
+        upc[t, :8] = np.frombuffer(O.x25519_base(O.previous_scalar(k)), "<u4")
+        upc[t, 8:] = np.frombuffer(O.x25519_base(k), "<u4")
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    state = np.zeros(lanes * 40, np.int32)
+    ns = np.zeros(lanes, np.uint64)
+    r.ref_init_walk(P(state, C.c_int32), P(upc, C.c_uint32), lanes)
+    ed = np.frombuffer(O.ed25519_public(ed_seed), ">u4").astype(np.uint32)
+    nh = O.name_hash("lxmf.delivery")
+    nhw = [int.from_bytes(nh[0:4], "big"), int.from_bytes(nh[4:8], "big"), (nh[8] << 24) | (nh[9] << 16)]
+    w, m = O.prefix_words(O.prefix_parse(prefix))
+    want, mask = np.array(w, np.uint32), np.array(m, np.uint32)
+    hc = np.zeros(1, np.uint32)
+    hits = np.zeros(2 * 4096, np.uint64)
+    q = np.frombuffer(O.u8b(), "<u4").astype(np.uint32)
+
+    def run(iters: int) -> float:
+        return r.ref_bench_walk(workers, P(state, C.c_int32), P(ns, C.c_uint64), lanes, iters, P(ed, C.c_uint32),
+                                nhw[0], nhw[1], nhw[2], P(want, C.c_uint32), P(mask, C.c_uint32), P(hc, C.c_uint32),
+                                P(hits, C.c_uint64), 4096, P(q, C.c_uint32))
+
+    rate = run(1)
+    iters = max(1, int(rate * step_seconds / (lanes * r.ref_batch())))
+    for _ in range(warmup):
+        run(iters)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run(iters)
+    dt = time.perf_counter() - t0
+    keys = steps * lanes * iters * r.ref_batch()
+    return {"value": keys / dt, "unit": "keys/s", "cores": workers, "kind": "reference",
+            "sample": f"{steps} steps x {lanes} lanes x {iters} batches of {r.ref_batch()} keys; the reference's "
+                      f"src/gpu/common.h walk_thread compiled for the host, {workers} threads",
+            "ms_per_step": dt / steps * 1e3}
+
+
+def main() -> None:
+    a = parse()
+    world, rank, local = dist_setup()
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        prefix = _prefix()
+        ref = reference_cpu(prefix, a.steps, a.warmup)
+        line = {"metric": METRIC, "value": ref["value"], "unit": "keys/s", "n_gpus": a.gpus, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ref.get("ms_per_step"), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded ChaCha20 starts)",
+                "impl": "reference",
+                "config": {"workload": "plain search, host cores", "prefix": prefix, "batch": 64},
+                "cpu_baseline": {"value": ref["value"], "unit": "keys/s", "cores": ref["cores"],
+                                 "kind": ref["kind"], "sample": ref["sample"]},
+                "e2e": {"value": ref["value"], "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import lxmfv as lx
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = local
+    torch.cuda.set_device(dev)
+    # A stream of our own (never the legacy default stream, whose handle is 0):
+    # the library launches on it and the timing events are recorded on it.
+    stream = torch.cuda.Stream(device=dev)
+    b = lx.Backend(device=dev, lanes=0, batch=a.batch, block=a.block, stream=stream.cuda_stream)
+    wave = b.threads()
+    b.close()
+    lanes = a.lanes or wave * max(1, -(-131072 // wave))
+    b = lx.Backend(device=dev, lanes=lanes, batch=a.batch, block=a.block, stream=stream.cuda_stream)
+
+    prefix = _prefix()
+    setup = lx.seeded_setup(SEED + 1000 * rank, lanes)
+    t0 = time.perf_counter()
+    b.init_from_scalars(setup.scalars)
+    ladder_s = time.perf_counter() - t0
+    per_iter = lanes * a.batch
+    iters = max(1, round(a.total_keys / (a.steps * per_iter)))
+    keys_per_step = per_iter * iters
+    args = lx.make_launch_args(iters, setup.ed_pub, lx.prefix_parse(prefix), max_hits=4096)
+
+    for _ in range(a.warmup):
+        b.launch_async(args)
+    b.collect()
+    kernel_ms_warm = b.last_kernel_ms()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            b.launch_async(args)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    kernel_ms_last = b.last_kernel_ms()
+    hits, n_hits = b.collect()
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_keys = keys_per_step * a.steps * world
+    value = total_keys / (ms * 1e-3)
+
+    # Every hit is rechecked from scratch on the CPU (OpenSSL), as the reference does.
+    pfx = lx.prefix_parse(prefix)
+    bad = [h for h in hits if not lx.prefix_matches(pfx, lx.address_of_identity(setup.identity(*h)))]
+
+    # End to end through the C ABI: synchronous lxmfv_launch per step, launch
+    # arguments from the host, hit count and hits read back every step.
+    e2e = None
+    if not a.no_e2e:
+        e2e_steps = max(1, a.steps // 2)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(e2e_steps):
+            h, _, _, n = b.launch(args)
+            d2h += 4 + 16 * len(h)
+        dt = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([dt], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        import ctypes
+        e2e = {"value": keys_per_step * e2e_steps * world / dt, "unit": "keys/s",
+               "h2d_bytes_per_step": ctypes.sizeof(lx.LaunchArgs), "d2h_bytes_per_step": d2h // e2e_steps,
+               "steps": e2e_steps, "api": "lxmfv_launch (C ABI, synchronous, host buffers)"}
+
+    imad_peak = b.peak_probe(0, 300.0)
+    alu_peak = b.peak_probe(2, 300.0)
+    kernel_s = ms * 1e-3 / a.steps
+    prods = wide_products_per_key(a.batch)
+    achieved = 2 * prods * keys_per_step / kernel_s  # lo + hi IMAD per 32x32->64 product
+    line = {
+        "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded ChaCha20 starts)",
+        "config": {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, B=64, 2^36 keys per run)",
+                   "prefix": prefix, "lanes_per_gpu": lanes, "batch": a.batch, "iters_per_step": iters,
+                   "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
+                   "l2": "working set (lane state + per-lane batch buffers) exceeds L2; no flush needed"},
+        "gpu_launches": a.steps,
+        "e2e": e2e,
+        "roofline": {"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
+                     "frac": achieved / imad_peak, "traffic": None,
+                     "note": f"algorithmic {2 * prods:.0f} IMAD (lo+hi of {prods:.0f} 32x32->64 products) per key; "
+                             f"peak = measured mad.lo.u32 rate of this GPU (probe)",
+                     "alu_peak_T": alu_peak / 1e12},
+        "clocks": clk.summary(),
+        "hits": {"found": int(n_hits), "rechecked_bad": len(bad)},
+        "start_points_s": ladder_s,
+        "kernel_ms": {"warm_last": kernel_ms_warm, "timed_last": kernel_ms_last},
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port(prefix)
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if bad:
+        sys.exit(f"{len(bad)} GPU hits failed their CPU recheck")
+
+
+def _prefix() -> str:
+    """The workload's 8-hex-digit prefix: numpy's default_rng(SEED)."""
+    import numpy as np
+    rng = np.random.default_rng(SEED)
+    return "".join("0123456789abcdef"[x] for x in rng.integers(0, 16, 8))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * liblxmfv: the B200-native (sm_100a) key-walk search of lxmf-vanity behind a
+ * plain C ABI.
+ *
+ * The reference (alaistair76/lxmf-vanity) reaches its GPU through the Rust
+ * trait `Backend` (src/gpu/mod.rs:41-52) and the CUDA entry points
+ * `init_walk` / `walk` (src/gpu/kernel.cu:21-36).  The functions below are
+ * what a Rust `Backend` implementation (or any other FFI) binds instead:
+ * plain pointers and sizes, no CUDA or C++ types, errors returned as codes
+ * with a message, never an abort.  One handle belongs to one host thread at a
+ * time; there is no hidden global state.
+ *
+ * Packing conventions follow the reference:
+ *   - public keys / u-coordinates: 8 little-endian uint32 words (32 LE bytes);
+ *   - the Ed25519 public key: 8 big-endian words (mod.rs:110);
+ *   - the name hash: 3 big-endian words, bytes 8-9 in the top half of the
+ *     third word (mod.rs:113-117);
+ *   - want / mask: 4 big-endian words of the destination hash (mod.rs:74-84);
+ *   - a hit is (walker lane, walk index n): the identity is
+ *     step_scalar(start[lane], n) || ed25519 seed (mod.rs:139-144).
+ */
+#ifndef LXMFV_H
+#define LXMFV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. */
+#define LXMFV_OK 0
+#define LXMFV_ERR_ARG -1     /* a bad argument (null pointer, size, range) */
+#define LXMFV_ERR_CUDA -2    /* the CUDA runtime or driver reported an error */
+#define LXMFV_ERR_NOMEM -3   /* a host or device allocation failed */
+#define LXMFV_ERR_STATE -4   /* the call is not valid in the handle's state */
+#define LXMFV_ERR_RECHECK -5 /* a GPU hit failed its from-scratch CPU recheck */
+#define LXMFV_ERR_OVERFLOW -6 /* more hits than the caller's buffer holds */
+
+typedef struct lxmfv_handle lxmfv_handle;
+
+/* Opening options; zero fields take defaults.
+ * Replaces the constants of src/gpu/cuda.rs:13-16 (BATCH, BLOCK,
+ * THREADS_PER_SM) and CudaContext::new(0) (cuda.rs:33-64). */
+typedef struct {
+    int32_t device;       /* CUDA device ordinal */
+    uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
+    uint32_t batch;       /* keys per batch inversion B: 16, 32, 64 or 128; 0: 64 */
+    uint32_t block;       /* threads per block: 128 or 256; 0: 256 */
+    void* stream;         /* cudaStream_t to launch on; NULL: a stream of the handle's own */
+} lxmfv_options;
+
+/* One launch of the walk.  Mirrors LaunchArgs (src/gpu/mod.rs:29-38). */
+typedef struct {
+    uint32_t iters;        /* batches of B keys per lane in this launch */
+    uint32_t ed[8];        /* Ed25519 public key, big-endian words */
+    uint32_t name_hash[3]; /* name hash, big-endian words */
+    uint32_t want[4];      /* destination-hash prefix, big-endian words */
+    uint32_t mask[4];
+    uint32_t q[8];         /* u(8B), little-endian words: the fixed step point */
+    uint32_t max_hits;     /* hit slots filled at most (the reference uses 4096) */
+    uint32_t dump_threads; /* lanes whose first dump_keys public keys are written */
+    uint32_t dump_keys;    /* keys dumped per lane; 0: B (the reference's dump) */
+} lxmfv_launch_args;
+
+/* A hit: lane `thread` at walk index `n`.  The pair of src/gpu/cuda.rs:124-129. */
+typedef struct {
+    uint32_t thread;
+    uint32_t reserved;
+    uint64_t n;
+} lxmfv_hit;
+
+/* Opens device `opts->device`, builds the walker state for `lanes` lanes and
+ * stores a handle in *out.  A handle is stored even on failure (when host
+ * memory allows), so that lxmfv_last_error can say why; close it either way.
+ * Replaces Cuda::new (src/gpu/cuda.rs:33-64). */
+int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out);
+
+/* The last error message of the handle ("" after success). */
+const char* lxmfv_last_error(const lxmfv_handle* h);
+
+/* "NVIDIA B200 (CUDA, compute 10.0, 148 SMs)"-style line.  Replaces
+ * Backend::describe (mod.rs:43). Returns the full length (snprintf-style). */
+int lxmfv_describe(const lxmfv_handle* h, char* buf, size_t len);
+
+/* Walker lanes: Backend::threads (mod.rs:44). */
+uint32_t lxmfv_threads(const lxmfv_handle* h);
+
+/* Keys per batch inversion: Backend::batch (mod.rs:46). */
+uint64_t lxmfv_batch(const lxmfv_handle* h);
+
+/* Sets every lane from u(k-8) and u(k): 16 little-endian words per lane,
+ * n_words = 16 * lanes.  Walk indices restart at 0.  Replaces Backend::init
+ * (mod.rs:48) / Cuda::init (cuda.rs:84-91) and the init_walk kernel
+ * (kernel.cu:21-24). */
+int lxmfv_init(lxmfv_handle* h, const uint32_t* u_prev_cur, size_t n_words);
+
+/* Sets every lane from its start scalar k (32 little-endian bytes per lane,
+ * n_bytes = 32 * lanes; clamped, with room to step, as random_start_scalar
+ * makes them, main.rs:157-171) by a Montgomery ladder on the GPU.  Replaces
+ * first_public_keys (mod.rs:212-228), which runs two X25519 per lane on the
+ * CPU, followed by Backend::init. */
+int lxmfv_init_from_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t n_bytes);
+
+/* Runs one launch of the walk and waits for it: every lane walks
+ * args->iters * B keys from where it stopped.  Writes up to `hits_cap` hits
+ * to `hits` and their total count (which may exceed hits_cap and
+ * args->max_hits) to *n_hits; when `dump` is not NULL, writes
+ * dump_threads * dump_keys * 8 public-key words (lane-major), and when
+ * `dump_addr` is not NULL, the matching 4-word destination hashes.
+ * Replaces Backend::launch (mod.rs:50-51) / Cuda::launch (cuda.rs:93-132) and
+ * the walk kernel (kernel.cu:26-36). */
+int lxmfv_launch(lxmfv_handle* h, const lxmfv_launch_args* args, lxmfv_hit* hits, uint32_t hits_cap,
+                 uint32_t* n_hits, uint32_t* dump, uint32_t* dump_addr);
+
+/* The asynchronous half of lxmfv_launch: enqueues the walk on the handle's
+ * stream and returns.  Hits accumulate on the device until lxmfv_collect.
+ * No counterpart in the reference (its launch always synchronises,
+ * cuda.rs:122); used to keep the walk back to back on the GPU. */
+int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args);
+
+/* Waits for the handle's stream, copies back up to hits_cap hits (and the
+ * dump of the last dumping launch), and clears the device hit queue. */
+int lxmfv_collect(lxmfv_handle* h, lxmfv_hit* hits, uint32_t hits_cap, uint32_t* n_hits, uint32_t* dump,
+                  uint32_t* dump_addr);
+
+/* Device time of the last walk kernel, in milliseconds (CUDA events on the
+ * launching stream; valid after lxmfv_launch or lxmfv_collect). */
+float lxmfv_last_kernel_ms(const lxmfv_handle* h);
+
+/* Releases the handle and its device memory (NULL is ignored). */
+void lxmfv_close(lxmfv_handle* h);
+
+/* ---- Host helpers (CPU): the reference's address and scalar rules. ---- */
+
+/* Prefix::parse (main.rs:206-216): 1..32 hex digits, any case; odd lengths
+ * are padded with '0'.  Writes 16 prefix bytes and returns the nibble count,
+ * or LXMFV_ERR_ARG. */
+int lxmfv_prefix_parse(const char* text, uint8_t bytes[16]);
+
+/* Prefix::matches (main.rs:218-224). */
+int lxmfv_prefix_matches(const uint8_t bytes[16], int nibbles, const uint8_t address[16]);
+
+/* prefix_words (mod.rs:74-84): big-endian want / mask words. */
+void lxmfv_prefix_words(const uint8_t bytes[16], int nibbles, uint32_t want[4], uint32_t mask[4]);
+
+/* name_hash (main.rs:174-176) of an aspect string, e.g. "lxmf.delivery". */
+void lxmfv_name_hash(const char* aspect, uint8_t out[10]);
+
+/* step_scalar (main.rs:125-137): k + 8n, little-endian. */
+void lxmfv_step_scalar(const uint8_t k[32], uint64_t n, uint8_t out[32]);
+
+/* previous_scalar (main.rs:140-152): k - 8. */
+void lxmfv_previous_scalar(const uint8_t k[32], uint8_t out[32]);
+
+/* Clamps k in place as random_start_scalar does (main.rs:161-163) and returns
+ * 1 when it also passes its rejection rule (main.rs:164-169), else 0. */
+int lxmfv_clamp_start(uint8_t k[32]);
+
+/* Seeded draws: the ChaCha20 keystream (RFC 8439 block function; key = seed
+ * as a u64 little-endian in bytes 0-7, zeros elsewhere; nonce 0; counter
+ * from 0).  An identity is the first accepted 32-byte scalar draw followed by
+ * the next 32 bytes (the Ed25519 seed); further scalars are further accepted
+ * draws.  Returns the stream offset after the draws. */
+uint64_t lxmfv_seeded_identity(uint64_t seed, uint8_t identity[64]);
+uint64_t lxmfv_seeded_scalars(uint64_t seed, uint64_t offset, uint8_t* scalars, uint64_t count);
+
+/* Fresh randomness from the operating system (getrandom), as the reference
+ * draws it (main.rs:160, main.rs:294, mod.rs:103). */
+int lxmfv_os_random(uint8_t* out, size_t len);
+
+/* Ed25519 public key of a 32-byte seed (SigningKey::verifying_key). */
+int lxmfv_ed25519_public(const uint8_t seed[32], uint8_t out[32]);
+
+/* x25519(k, 9): the X25519 public key of a private key (clamps k). */
+int lxmfv_x25519_base(const uint8_t k[32], uint8_t out[32]);
+
+/* address_of_identity (main.rs:191-197), computed from scratch on the CPU with
+ * an independent implementation (OpenSSL): the recheck every hit passes. */
+int lxmfv_address_of_identity(const uint8_t identity[64], const uint8_t name_hash[10], uint8_t out[16]);
+
+/* ---- Primitive kernels (the field and hash microbench). ---- */
+
+/* Field op on `count` elements of 8 little-endian words on the GPU: inputs
+ * drop bit 255 (fe_from_words, common.h:131-142), outputs are canonical
+ * (fe_to_words, common.h:145-174).  op 0: a*b (fe_mul, common.h:75-89);
+ * 1: a^2 (fe_sq, common.h:92-107); 2: a^(p-2) (fe_invert, common.h:115-128);
+ * 3: batch inversion by Montgomery's trick over groups of `group` elements
+ * (common.h:326-356).  Host buffers; returns LXMFV_OK. */
+int lxmfv_fe_op(lxmfv_handle* h, int op, const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t count,
+                uint32_t group);
+
+/* The destination-hash chain on `count` 64-byte public keys (32 LE u bytes
+ * then 32 key bytes) with one name hash: 16-byte outputs.  The three
+ * compressions of lxmf_address (common.h:221-253).  Host buffers. */
+int lxmfv_address_chain(lxmfv_handle* h, const uint8_t* pks, const uint8_t name_hash[10], uint8_t* out,
+                        uint64_t count);
+
+/* Integer-pipe throughput probe: runs `kind` (0: IMAD, 1: IMAD.HI-class
+ * mad.hi, 2: LOP3/IADD3/SHF mix) on every SM for about `ms` milliseconds and
+ * returns lane-operations per second in *ops_per_s.  Diagnostic with no
+ * counterpart in the reference: the denominator of the integer roofline. */
+int lxmfv_peak_probe(lxmfv_handle* h, int kind, float ms, double* ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LXMFV_H */

@@ -1,0 +1,461 @@
+// liblxmfv: the C ABI of include/lxmfv.h over the sm_100a kernels.
+//
+// Replaces the reference's CUDA backend (src/gpu/cuda.rs): where that
+// compiles common.h with NVRTC at start-up and, on every launch, copies four
+// small arrays to the device and allocates three buffers (cuda.rs:93-101),
+// this library is compiled ahead of time for sm_100a, passes the launch
+// arguments by value in the kernel's parameter block, and keeps the hit
+// queue and dump buffers allocated for the handle's lifetime.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/lxmfv.h"
+#include "walk_kernels.cuh"
+
+struct lxmfv_handle {
+    int device = 0;
+    int sms = 0;
+    int cc_major = 0, cc_minor = 0;
+    std::string name;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t lanes = 0;
+    uint32_t batch = 64;
+    uint32_t block = 256;
+    uint32_t* d_state = nullptr;
+    uint64_t* d_ns = nullptr;
+    uint32_t* d_hit_count = nullptr;
+    lxk::Hit* d_hits = nullptr;
+    uint32_t hits_cap = 0;
+    uint32_t* d_dump_u = nullptr;
+    uint32_t* d_dump_addr = nullptr;
+    size_t dump_cap_keys = 0;
+    uint32_t dump_lanes = 0, dump_keys = 0;  // of the last dumping launch
+    uint32_t launch_max_hits = 0;            // largest max_hits since the last collect
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+    bool initialised = false;
+    std::string err;
+};
+
+namespace {
+
+int fail(lxmfv_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    return code;
+}
+
+#define CU(h, call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail((h), LXMFV_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                 \
+    } while (0)
+
+typedef void (*walk_fn)(lxk::WalkArgs);
+
+template <int B, int BLOCK>
+walk_fn walk_for() {
+    return lxk::walk_kernel<B, BLOCK, (BLOCK == 256 ? 2 : 4)>;
+}
+
+walk_fn pick_walk(uint32_t batch, uint32_t block) {
+#define LXMFV_CASE(B)                                                 \
+    if (batch == B) return block == 128 ? walk_for<B, 128>() : walk_for<B, 256>();
+    LXMFV_CASE(16)
+    LXMFV_CASE(32)
+    LXMFV_CASE(64)
+    LXMFV_CASE(128)
+#undef LXMFV_CASE
+    return nullptr;
+}
+
+// SHA-256 rounds 0 and 1 of the destination block, which see only the name
+// hash: the same for every key of a search.
+void block3_head(const uint32_t nh[3], uint32_t head[8]) {
+    static const uint32_t K0 = 0x428a2f98u, K1 = 0x71374491u;
+    auto rotr = [](uint32_t x, int n) { return (x >> n) | (x << (32 - n)); };
+    uint32_t a = 0x6a09e667u, b = 0xbb67ae85u, c = 0x3c6ef372u, d = 0xa54ff53au;
+    uint32_t e = 0x510e527fu, f = 0x9b05688cu, g = 0x1f83d9abu, hh = 0x5be0cd19u;
+    const uint32_t kw[2] = {K0 + nh[0], K1 + nh[1]};
+    for (int i = 0; i < 2; i++) {
+        const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + kw[i];
+        const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+        hh = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+    }
+    head[0] = a; head[1] = b; head[2] = c; head[3] = d; head[4] = e; head[5] = f; head[6] = g; head[7] = hh;
+}
+
+void fill_addr_consts(lxsha::AddrConsts& ac, const uint32_t ed[8], const uint32_t nh[3], const uint32_t want[4],
+                      const uint32_t mask[4]) {
+    for (int i = 0; i < 8; i++) ac.ed[i] = ed ? ed[i] : 0;
+    for (int i = 0; i < 3; i++) ac.nh[i] = nh[i];
+    block3_head(nh, ac.head);
+    for (int i = 0; i < 4; i++) {
+        ac.want[i] = want ? want[i] : 0;
+        ac.mask[i] = mask ? mask[i] : 0;
+    }
+}
+
+int ensure_hits(lxmfv_handle* h, uint32_t cap) {
+    if (cap <= h->hits_cap) return LXMFV_OK;
+    // Grow only between launches: every queued launch has finished here.
+    CU(h, cudaStreamSynchronize(h->stream));
+    lxk::Hit* nh = nullptr;
+    CU(h, cudaMalloc(&nh, sizeof(lxk::Hit) * cap));
+    if (h->d_hits) {
+        CU(h, cudaMemcpyAsync(nh, h->d_hits, sizeof(lxk::Hit) * h->hits_cap, cudaMemcpyDeviceToDevice, h->stream));
+        CU(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->d_hits);
+    }
+    h->d_hits = nh;
+    h->hits_cap = cap;
+    return LXMFV_OK;
+}
+
+int ensure_dump(lxmfv_handle* h, size_t keys) {
+    if (keys <= h->dump_cap_keys) return LXMFV_OK;
+    CU(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_dump_u);
+    cudaFree(h->d_dump_addr);
+    h->d_dump_u = nullptr;
+    h->d_dump_addr = nullptr;
+    h->dump_cap_keys = 0;
+    CU(h, cudaMalloc(&h->d_dump_u, keys * 8 * sizeof(uint32_t)));
+    CU(h, cudaMalloc(&h->d_dump_addr, keys * 4 * sizeof(uint32_t)));
+    h->dump_cap_keys = keys;
+    return LXMFV_OK;
+}
+
+int set_device(lxmfv_handle* h) {
+    CU(h, cudaSetDevice(h->device));
+    return LXMFV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
+    if (!out) return LXMFV_ERR_ARG;
+    *out = nullptr;
+    lxmfv_handle* h = new (std::nothrow) lxmfv_handle();
+    if (!h) return LXMFV_ERR_NOMEM;
+    *out = h;
+    lxmfv_options o{};
+    if (opts) o = *opts;
+    h->device = o.device;
+    h->batch = o.batch ? o.batch : 64;
+    h->block = o.block ? o.block : 256;
+    if (!pick_walk(h->batch, h->block) || (h->block != 128 && h->block != 256))
+        return fail(h, LXMFV_ERR_ARG, "unsupported batch %u / block %u (batch 16, 32, 64, 128; block 128, 256)",
+                    h->batch, h->block);
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(h, LXMFV_ERR_CUDA, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "none found");
+    if (h->device < 0 || h->device >= count)
+        return fail(h, LXMFV_ERR_ARG, "device %d out of range (%d devices)", h->device, count);
+    if (int rc = set_device(h)) return rc;
+    cudaDeviceProp prop;
+    CU(h, cudaGetDeviceProperties(&prop, h->device));
+    h->sms = prop.multiProcessorCount;
+    h->cc_major = prop.major;
+    h->cc_minor = prop.minor;
+    h->name = prop.name;
+    if (prop.major != 10 || prop.minor != 0)
+        return fail(h, LXMFV_ERR_CUDA, "%s is compute %d.%d; this library is built for sm_100a (B200) only", prop.name,
+                    prop.major, prop.minor);
+    if (o.stream) {
+        h->stream = (cudaStream_t)o.stream;
+    } else {
+        CU(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->own_stream = true;
+    }
+    CU(h, cudaEventCreate(&h->ev0));
+    CU(h, cudaEventCreate(&h->ev1));
+    walk_fn fn = pick_walk(h->batch, h->block);
+    int per_sm = 0;
+    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)h->block, 0));
+    if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
+    h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;
+    CU(h, cudaMalloc(&h->d_state, (size_t)h->lanes * 32 * sizeof(uint32_t)));
+    CU(h, cudaMalloc(&h->d_ns, (size_t)h->lanes * sizeof(uint64_t)));
+    CU(h, cudaMalloc(&h->d_hit_count, sizeof(uint32_t)));
+    CU(h, cudaMemsetAsync(h->d_hit_count, 0, sizeof(uint32_t), h->stream));
+    CU(h, cudaMemsetAsync(h->d_state, 0, (size_t)h->lanes * 32 * sizeof(uint32_t), h->stream));
+    CU(h, cudaMemsetAsync(h->d_ns, 0, (size_t)h->lanes * sizeof(uint64_t), h->stream));
+    if (int rc = ensure_hits(h, 4096)) return rc;
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+const char* lxmfv_last_error(const lxmfv_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int lxmfv_describe(const lxmfv_handle* h, char* buf, size_t len) {
+    if (!h) return LXMFV_ERR_ARG;
+    return snprintf(buf, len, "%s (CUDA, compute %d.%d, %d SMs)", h->name.c_str(), h->cc_major, h->cc_minor, h->sms);
+}
+
+uint32_t lxmfv_threads(const lxmfv_handle* h) { return h ? h->lanes : 0; }
+
+uint64_t lxmfv_batch(const lxmfv_handle* h) { return h ? h->batch : 0; }
+
+int lxmfv_init(lxmfv_handle* h, const uint32_t* u_prev_cur, size_t n_words) {
+    if (!h || !u_prev_cur) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (!h->d_state) return fail(h, LXMFV_ERR_STATE, "handle is not open");
+    if (n_words != (size_t)h->lanes * 16)
+        return fail(h, LXMFV_ERR_ARG, "u_prev_cur has %zu words; %u lanes need %zu", n_words, h->lanes,
+                    (size_t)h->lanes * 16);
+    if (int rc = set_device(h)) return rc;
+    uint32_t* d = nullptr;
+    CU(h, cudaMalloc(&d, n_words * sizeof(uint32_t)));
+    cudaError_t e = cudaMemcpyAsync(d, u_prev_cur, n_words * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        lxk::init_kernel<<<(h->lanes + 255) / 256, 256, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "init: %s", cudaGetErrorString(e));
+    h->initialised = true;
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+int lxmfv_init_from_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t n_bytes) {
+    if (!h || !scalars) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (!h->d_state) return fail(h, LXMFV_ERR_STATE, "handle is not open");
+    if (n_bytes != (size_t)h->lanes * 32)
+        return fail(h, LXMFV_ERR_ARG, "scalars have %zu bytes; %u lanes need %zu", n_bytes, h->lanes,
+                    (size_t)h->lanes * 32);
+    for (size_t t = 0; t < h->lanes; t++) {
+        const uint8_t* k = scalars + 32 * t;
+        if ((k[0] & 7) != 0 || (k[31] & 0xC0) != 0x40)
+            return fail(h, LXMFV_ERR_ARG, "scalar %zu is not clamped (k mod 8 = 0, bit 254 set, bit 255 clear)", t);
+    }
+    if (int rc = set_device(h)) return rc;
+    uint32_t* d = nullptr;
+    CU(h, cudaMalloc(&d, n_bytes));
+    cudaError_t e = cudaMemcpyAsync(d, scalars, n_bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        fe q;
+        // u(8B), the fixed step point (mod.rs:111, main.rs:244).
+        static const uint32_t U8B[8] = {0x48c99968u, 0xf1716fedu, 0xad74a91eu, 0x7a78edcau,
+                                        0xc8b65ca1u, 0xd83b884du, 0xaad65c2du, 0x275fa6d7u};
+        for (int i = 0; i < 8; i++) q.v[i] = U8B[i];
+        lxk::ladder_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes, q);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "init_from_scalars: %s", cudaGetErrorString(e));
+    h->initialised = true;
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args) {
+    if (!h || !args) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (!h->initialised) return fail(h, LXMFV_ERR_STATE, "launch before init");
+    if (args->iters == 0) return fail(h, LXMFV_ERR_ARG, "iters must be at least 1");
+    if (int rc = set_device(h)) return rc;
+    lxk::WalkArgs wa;
+    memset(&wa, 0, sizeof wa);
+    wa.state = h->d_state;
+    wa.ns = h->d_ns;
+    wa.lanes = h->lanes;
+    wa.iters = args->iters;
+    for (int i = 0; i < 8; i++) wa.q.v[i] = args->q[i];
+    wa.q.v[7] &= 0x7fffffffu;
+    fill_addr_consts(wa.ac, args->ed, args->name_hash, args->want, args->mask);
+    if (int rc = ensure_hits(h, std::max<uint32_t>(args->max_hits, 1))) return rc;
+    wa.hit_count = h->d_hit_count;
+    wa.hits = h->d_hits;
+    wa.max_hits = args->max_hits;
+    h->launch_max_hits = std::max(h->launch_max_hits, args->max_hits);
+    if (args->dump_threads > 0) {
+        const uint32_t dl = std::min(args->dump_threads, h->lanes);
+        const uint32_t dk = args->dump_keys ? args->dump_keys : h->batch;
+        if ((uint64_t)dk > (uint64_t)args->iters * h->batch)
+            return fail(h, LXMFV_ERR_ARG, "dump_keys %u exceeds the %llu keys a lane walks in this launch", dk,
+                        (unsigned long long)args->iters * h->batch);
+        if (int rc = ensure_dump(h, (size_t)dl * dk)) return rc;
+        wa.dump_lanes = dl;
+        wa.dump_keys = dk;
+        wa.dump_u = h->d_dump_u;
+        wa.dump_addr = h->d_dump_addr;
+        h->dump_lanes = dl;
+        h->dump_keys = dk;
+    }
+    walk_fn fn = pick_walk(h->batch, h->block);
+    CU(h, cudaEventRecord(h->ev0, h->stream));
+    fn<<<(h->lanes + h->block - 1) / h->block, h->block, 0, h->stream>>>(wa);
+    CU(h, cudaGetLastError());
+    CU(h, cudaEventRecord(h->ev1, h->stream));
+    h->timed = true;
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+int lxmfv_collect(lxmfv_handle* h, lxmfv_hit* hits, uint32_t hits_cap, uint32_t* n_hits, uint32_t* dump,
+                  uint32_t* dump_addr) {
+    if (!h || !n_hits) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (int rc = set_device(h)) return rc;
+    CU(h, cudaStreamSynchronize(h->stream));
+    uint32_t count = 0;
+    CU(h, cudaMemcpy(&count, h->d_hit_count, sizeof count, cudaMemcpyDeviceToHost));
+    const uint32_t stored = std::min(std::min(count, h->launch_max_hits), h->hits_cap);
+    const uint32_t give = hits ? std::min(stored, hits_cap) : 0;
+    if (give > 0) CU(h, cudaMemcpy(hits, h->d_hits, sizeof(lxk::Hit) * give, cudaMemcpyDeviceToHost));
+    const size_t dumped = (size_t)h->dump_lanes * h->dump_keys;
+    if (dump && dumped) CU(h, cudaMemcpy(dump, h->d_dump_u, dumped * 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (dump_addr && dumped)
+        CU(h, cudaMemcpy(dump_addr, h->d_dump_addr, dumped * 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CU(h, cudaMemsetAsync(h->d_hit_count, 0, sizeof(uint32_t), h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->launch_max_hits = 0;
+    h->dump_lanes = 0;
+    h->dump_keys = 0;
+    *n_hits = count;
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+int lxmfv_launch(lxmfv_handle* h, const lxmfv_launch_args* args, lxmfv_hit* hits, uint32_t hits_cap,
+                 uint32_t* n_hits, uint32_t* dump, uint32_t* dump_addr) {
+    if (int rc = lxmfv_launch_async(h, args)) return rc;
+    return lxmfv_collect(h, hits, hits_cap, n_hits, dump, dump_addr);
+}
+
+float lxmfv_last_kernel_ms(const lxmfv_handle* h) {
+    if (!h || !h->timed) return -1.0f;
+    float ms = -1.0f;
+    if (cudaEventSynchronize(h->ev1) != cudaSuccess) return -1.0f;
+    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) != cudaSuccess) return -1.0f;
+    return ms;
+}
+
+void lxmfv_close(lxmfv_handle* h) {
+    if (!h) return;
+    if (h->sms) {
+        cudaSetDevice(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        cudaFree(h->d_state);
+        cudaFree(h->d_ns);
+        cudaFree(h->d_hit_count);
+        cudaFree(h->d_hits);
+        cudaFree(h->d_dump_u);
+        cudaFree(h->d_dump_addr);
+        if (h->ev0) cudaEventDestroy(h->ev0);
+        if (h->ev1) cudaEventDestroy(h->ev1);
+        if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+}
+
+// ---- Primitive kernels.
+
+int lxmfv_fe_op(lxmfv_handle* h, int op, const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t count,
+                uint32_t group) {
+    if (!h || !a || !out || (op == 0 && !b)) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (op < 0 || op > 3) return fail(h, LXMFV_ERR_ARG, "op %d: 0 mul, 1 square, 2 invert, 3 batch invert", op);
+    if (op == 3 && (group < 1 || group > 256)) return fail(h, LXMFV_ERR_ARG, "group %u not in 1..256", group);
+    if (count == 0) return LXMFV_OK;
+    if (int rc = set_device(h)) return rc;
+    const size_t bytes = count * 8 * sizeof(uint32_t);
+    uint32_t *da = nullptr, *db = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&da, bytes);
+    if (e == cudaSuccess && op == 0) e = cudaMalloc(&db, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(da, a, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && op == 0) e = cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        const int grid = h->sms * 8;
+        if (op == 3) {
+            lxk::fe_batch_invert_kernel<<<grid, 128, 0, h->stream>>>(da, dout, count, group);
+        } else {
+            lxk::fe_op_kernel<<<grid, 256, 0, h->stream>>>(op, da, db, dout, count);
+        }
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "fe_op: %s", cudaGetErrorString(e));
+    return LXMFV_OK;
+}
+
+int lxmfv_address_chain(lxmfv_handle* h, const uint8_t* pks, const uint8_t name_hash[10], uint8_t* out,
+                        uint64_t count) {
+    if (!h || !pks || !name_hash || !out) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (count == 0) return LXMFV_OK;
+    if (int rc = set_device(h)) return rc;
+    uint32_t nh[3] = {(uint32_t)name_hash[0] << 24 | (uint32_t)name_hash[1] << 16 | (uint32_t)name_hash[2] << 8 | name_hash[3],
+                      (uint32_t)name_hash[4] << 24 | (uint32_t)name_hash[5] << 16 | (uint32_t)name_hash[6] << 8 | name_hash[7],
+                      (uint32_t)name_hash[8] << 24 | (uint32_t)name_hash[9] << 16};
+    lxsha::AddrConsts ac;
+    fill_addr_consts(ac, nullptr, nh, nullptr, nullptr);
+    uint32_t *dpk = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&dpk, count * 64);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, count * 16);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dpk, pks, count * 64, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        lxk::address_chain_kernel<<<h->sms * 8, 256, 0, h->stream>>>(dpk, ac, dout, count);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, count * 16, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dpk);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "address_chain: %s", cudaGetErrorString(e));
+    return LXMFV_OK;
+}
+
+int lxmfv_peak_probe(lxmfv_handle* h, int kind, float ms, double* ops_per_s) {
+    if (!h || !ops_per_s || kind < 0 || kind > 2) return fail(h, LXMFV_ERR_ARG, "bad argument");
+    if (int rc = set_device(h)) return rc;
+    uint32_t* sink = nullptr;
+    CU(h, cudaMalloc(&sink, sizeof(uint32_t)));
+    const int blocks = h->sms * 8, threads = 256;
+    const double per_iter = (double)blocks * threads * 16 * 8 * (kind == 2 ? 2 : 1);
+    uint32_t iters = 64;
+    float t = 0;
+    cudaError_t e = cudaSuccess;
+    for (int pass = 0; pass < 4 && e == cudaSuccess; pass++) {
+        e = cudaEventRecord(h->ev0, h->stream);
+        if (e == cudaSuccess) {
+            lxk::probe_kernel<<<blocks, threads, 0, h->stream>>>(kind, iters, 12345u + pass, sink);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev1, h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(h->ev1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, h->ev0, h->ev1);
+        if (e != cudaSuccess) break;
+        if (pass < 3 && t > 0) {
+            const double want = std::max(ms, 1.0f);
+            iters = (uint32_t)std::min(1e7, std::max(1.0, iters * want / t));
+        }
+    }
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "peak_probe: %s", cudaGetErrorString(e));
+    *ops_per_s = per_iter * iters / (t * 1e-3);
+    return LXMFV_OK;
+}
+
+}  // extern "C"

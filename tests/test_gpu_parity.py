@@ -1,0 +1,246 @@
+"""Parity of the sm_100a kernels with the oracle, through the C ABI.
+
+Bit-exact throughout: field primitives (mul, square, invert, batch
+inversion) and the destination-hash chain against the golden fixtures;
+public keys of the GPU ladder and of the walk against plain X25519; every
+hit of the walk against the oracle's search; the seed-1 single-search window
+(2^24 keys, prefix b00b1) split over lanes against its fixture."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _keys_of(dump: np.ndarray, lanes: int, keys: int) -> np.ndarray:
+    return dump.reshape(lanes, keys, 8).view(np.uint8).reshape(lanes, keys, 32)
+
+
+def _hashes_of(dump_addr: np.ndarray, lanes: int, keys: int) -> np.ndarray:
+    return dump_addr.reshape(lanes, keys, 4).astype(">u4").view(np.uint8).reshape(lanes, keys, 16)
+
+
+def test_describe(backend):
+    d = backend.describe()
+    assert "compute 10.0" in d and "SMs" in d
+    assert backend.threads() == 4096 and backend.batch() == 64
+
+
+def test_field_small_golden(backend):
+    g = np.load(os.path.join(GOLDEN, "fe_small.npz"))
+    assert (backend.fe_op(0, g["a"], g["b"]) == g["mul"]).all()
+    assert (backend.fe_op(1, g["a"]) == g["sqr"]).all()
+    assert (backend.fe_op(2, g["a"]) == g["inv"]).all()
+    assert (backend.fe_op(3, g["a"], group=64) == g["binv"]).all()
+
+
+def test_field_digest(backend):
+    from tests.golden.inputs import fe_inputs
+    d = json.load(open(os.path.join(GOLDEN, "fe_digest.json")))
+    a, b = fe_inputs(d["count"])
+    dig = lambda x: hashlib.sha256(np.ascontiguousarray(x).tobytes()).hexdigest()  # noqa: E731
+    assert dig(backend.fe_op(0, a, b)) == d["mul"]
+    assert dig(backend.fe_op(1, a)) == d["sqr"]
+    assert dig(backend.fe_op(2, a)) == d["inv"]
+    assert dig(backend.fe_op(3, a, group=64)) == d["binv"]
+
+
+def test_field_random_256bit_inputs(backend, oracle):
+    """Full 256-bit inputs (bit 255 set included) against the oracle."""
+    rng = np.random.default_rng(31)
+    a = rng.integers(0, 2**32, size=(1 << 14, 8), dtype=np.uint64).astype(np.uint32)
+    b = rng.integers(0, 2**32, size=(1 << 14, 8), dtype=np.uint64).astype(np.uint32)
+    a[:8] = 0xFFFFFFFF
+    b[4:12] = 0xFFFFFFFF
+    assert (backend.fe_op(0, a, b) == oracle.fe_op(0, a, b)).all()
+    assert (backend.fe_op(1, a) == oracle.fe_op(1, a)).all()
+    assert (backend.fe_op(2, a[:2048]) == oracle.fe_op(2, a[:2048])).all()
+    for g in (1, 7, 64, 256):
+        assert (backend.fe_op(3, a[:2048], group=g) == oracle.fe_batch_invert(a[:2048], g)).all(), g
+
+
+def test_address_chain(backend, oracle):
+    from tests.golden.inputs import chain_inputs
+    g = np.load(os.path.join(GOLDEN, "chain_small.npz"))
+    nh = oracle.name_hash("lxmf.delivery")
+    assert (backend.address_chain(g["pks"], nh) == g["out"]).all()
+    d = json.load(open(os.path.join(GOLDEN, "chain_digest.json")))
+    out = backend.address_chain(chain_inputs(d["count"]), nh)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == d["sha256"]
+    pks = chain_inputs(512)
+    for aspect in ("nomadnetwork.node", "lxmf.propagation"):
+        nh2 = oracle.name_hash(aspect)
+        assert (backend.address_chain(pks, nh2) == oracle.address_chain(pks, nh2)).all()
+
+
+def _walk(backend, lx, setup, prefix, iters, dump_lanes=0, dump_keys=0, max_hits=4096, aspect="lxmf.delivery"):
+    args = lx.make_launch_args(iters, setup.ed_pub, lx.prefix_parse(prefix), aspect=aspect, max_hits=max_hits,
+                               dump_threads=dump_lanes, dump_keys=dump_keys)
+    return backend.launch(args, want_dump=dump_lanes > 0, want_dump_addr=dump_lanes > 0)
+
+
+def test_ladder_start_points_and_first_batch(backend, lx, oracle):
+    """GPU ladder starts: the first batch of every dumped lane equals
+    x25519(k + 8i) (the shape of the reference's self-test, mod.rs:183-193)."""
+    setup = lx.seeded_setup(101, backend.threads())
+    backend.init_from_scalars(setup.scalars)
+    hits, dump, dump_addr, n = _walk(backend, lx, setup, "b0", 1, dump_lanes=48)
+    keys = _keys_of(dump, 48, 64)
+    for t in range(48):
+        k = bytes(setup.scalars[t])
+        for i in range(0, 64, 3 if t > 2 else 1):
+            assert bytes(keys[t, i]) == oracle.x25519_base(oracle.step_scalar(k, i)), (t, i)
+    nh = oracle.name_hash()
+    hashes = _hashes_of(dump_addr, 48, 64)
+    for t in range(0, 48, 5):
+        for i in range(64):
+            assert bytes(hashes[t, i]) == oracle.lxmf_address(nh, bytes(keys[t, i]), setup.ed_pub)
+
+
+def test_reference_init_interface(backend, lx, oracle):
+    """Backend::init from u(k-8), u(k) words gives the same walk as the ladder."""
+    lanes = backend.threads()
+    setup = lx.seeded_setup(202, lanes)
+    upc = np.zeros((lanes, 16), np.uint32)
+    for t in range(lanes):
+        k = bytes(setup.scalars[t])
+        if t < 16:
+            upc[t, :8] = np.frombuffer(oracle.x25519_base(oracle.previous_scalar(k)), "<u4")
+            upc[t, 8:] = np.frombuffer(oracle.x25519_base(k), "<u4")
+    backend.init(upc)
+    _, dump_a, _, _ = _walk(backend, lx, setup, "b0", 2, dump_lanes=16, dump_keys=128)
+    backend.init_from_scalars(setup.scalars)
+    _, dump_b, _, _ = _walk(backend, lx, setup, "b0", 2, dump_lanes=16, dump_keys=128)
+    assert (dump_a == dump_b).all()
+    keys = _keys_of(dump_a, 16, 128)
+    for t in range(16):
+        walked = oracle.walk_keys(bytes(setup.scalars[t]), 128)
+        assert (keys[t] == walked).all(), t
+
+
+def test_hits_match_oracle_search(backend, lx, oracle):
+    """Every hit of a 2-nibble search over 4096 lanes x 256 keys, exactly."""
+    lanes = backend.threads()
+    setup = lx.seeded_setup(303, lanes)
+    backend.init_from_scalars(setup.scalars)
+    hits, _, _, n = _walk(backend, lx, setup, "b0", 4, max_hits=1 << 16)
+    assert n == len(hits)
+    nh = oracle.name_hash()
+    pfx = oracle.prefix_parse("b0")
+    expected = set()
+    for t in range(lanes):
+        h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, nh, pfx, 256)
+        expected.update((t, int(x)) for x in h)
+    assert set(hits) == expected and len(hits) == len(expected)
+    assert 3000 < len(expected) < 5200  # 2^20 keys / 256
+
+
+def test_state_persists_across_launches(backend, lx, oracle):
+    """Two launches continue one walk: indices 0..63 then 64..127."""
+    setup = lx.seeded_setup(404, backend.threads())
+    backend.init_from_scalars(setup.scalars)
+    _, d1, _, _ = _walk(backend, lx, setup, "b0", 1, dump_lanes=4)
+    _, d2, _, _ = _walk(backend, lx, setup, "b0", 1, dump_lanes=4)
+    for t in range(4):
+        walked = oracle.walk_keys(bytes(setup.scalars[t]), 128)
+        assert (_keys_of(d1, 4, 64)[t] == walked[:64]).all()
+        assert (_keys_of(d2, 4, 64)[t] == walked[64:]).all()
+
+
+def test_config1_single_search_window(backend, lx):
+    """Config 1: seed 1, lxmf.delivery, walk indices [0, 2^24), prefix b00b1,
+    the walk split into 4096 lanes of 4096 keys.  All hits and the first 4096
+    destination hashes against the fixture (oracle and reference agreed)."""
+    c = json.load(open(os.path.join(GOLDEN, "config1.json")))
+    lanes = backend.threads()
+    per = c["keys"] // lanes
+    setup = lx.segmented_setup(bytes.fromhex(c["scalar"]), bytes.fromhex(c["ed_seed"]), lanes, per)
+    assert setup.ed_pub.hex() == c["ed_pub"]
+    backend.init_from_scalars(setup.scalars)
+    hits, _, dump_addr, n = _walk(backend, lx, setup, c["prefix"], per // 64, dump_lanes=1, dump_keys=4096)
+    got = sorted(t * per + k for t, k in hits)
+    assert got == c["hits"]
+    gold = np.fromfile(os.path.join(GOLDEN, "config1_dest4096.bin"), np.uint8).reshape(4096, 16)
+    assert (_hashes_of(dump_addr, 1, 4096)[0] == gold).all()
+    for t, k in hits:
+        assert lx.prefix_matches(lx.prefix_parse(c["prefix"]), lx.address_of_identity(setup.identity(t, k)))
+
+
+def test_full_length_prefix_finds_exactly_one_key(backend, lx, oracle):
+    """A 32-nibble prefix (the whole address) of one walked key: one hit."""
+    setup = lx.seeded_setup(505, backend.threads())
+    addr = oracle.lxmf_address(oracle.name_hash(), oracle.walk_keys(bytes(setup.scalars[7]), 200)[137].tobytes(),
+                               setup.ed_pub)
+    backend.init_from_scalars(setup.scalars)
+    hits, _, _, n = _walk(backend, lx, setup, addr.hex(), 4)
+    assert hits == [(7, 137)] and n == 1
+
+
+def test_hit_queue_overflow_is_counted(backend, lx):
+    setup = lx.seeded_setup(606, backend.threads())
+    backend.init_from_scalars(setup.scalars)
+    hits, _, _, n = _walk(backend, lx, setup, "b", 1, max_hits=5)
+    assert len(hits) == 5 and n > 10000  # 2^18 keys / 16
+    pfx = lx.prefix_parse("b")
+    for t, k in hits:
+        assert lx.prefix_matches(pfx, lx.address_of_identity(setup.identity(t, k)))
+
+
+@pytest.mark.parametrize("aspect", ["nomadnetwork.node", "lxmf.propagation"])
+def test_other_aspects(backend, lx, oracle, aspect):
+    setup = lx.seeded_setup(707, backend.threads())
+    backend.init_from_scalars(setup.scalars)
+    hits, _, _, _ = _walk(backend, lx, setup, "c3", 1, aspect=aspect, max_hits=1 << 14)
+    nh = oracle.name_hash(aspect)
+    expected = set()
+    for t in range(0, backend.threads()):
+        h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, nh, oracle.prefix_parse("c3"), 64)
+        expected.update((t, int(x)) for x in h)
+    assert set(hits) == expected
+
+
+@pytest.mark.parametrize("batch,block", [(16, 256), (32, 128), (128, 256)])
+def test_other_batch_sizes(lx, oracle, batch, block):
+    with lx.Backend(device=0, lanes=512, batch=batch, block=block) as b:
+        setup = lx.seeded_setup(808 + batch, 512)
+        b.init_from_scalars(setup.scalars)
+        args = lx.make_launch_args(2, setup.ed_pub, lx.prefix_parse("b0"), max_hits=1 << 14, dump_threads=3,
+                                   dump_keys=2 * batch)
+        hits, dump, _, n = b.launch(args, want_dump=True)
+        keys = _keys_of(dump, 3, 2 * batch)
+        for t in range(3):
+            assert (keys[t] == oracle.walk_keys(bytes(setup.scalars[t]), 2 * batch)).all()
+        expected = set()
+        for t in range(512):
+            h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, oracle.name_hash(),
+                                        oracle.prefix_parse("b0"), 2 * batch)
+            expected.update((t, int(x)) for x in h)
+        assert set(hits) == expected
+
+
+def test_self_test_shape(lx):
+    """The reference's --gpu-self-test (mod.rs:178-207) on the default-sized
+    device: the first batch of 256 lanes against plain X25519, >= 100 hits for
+    'b0' with iters = 1, every hit rechecked from scratch on the CPU."""
+    with lx.Backend(device=0) as b:
+        lanes = b.threads()
+        assert lanes >= 256
+        starts = np.stack([np.frombuffer(lx.random_start_scalar(), np.uint8) for _ in range(256)])
+        scal = np.concatenate([starts, lx.seeded_setup(909, lanes - 256).scalars])
+        b.init_from_scalars(scal)
+        seed = lx.os_random(32)
+        ed_pub = lx.ed25519_public(seed)
+        args = lx.make_launch_args(1, ed_pub, lx.prefix_parse("b0"), dump_threads=256)
+        hits, dump, _, n = b.launch(args, want_dump=True)
+        keys = _keys_of(dump, 256, b.batch())
+        for t in range(256):
+            for i in range(b.batch()):
+                assert bytes(keys[t, i]) == lx.x25519_base(lx.step_scalar(bytes(scal[t]), i))
+        assert len(hits) >= 100
+        pfx = lx.prefix_parse("b0")
+        for t, k in hits:
+            assert lx.prefix_matches(pfx, lx.address_of_identity(lx.step_scalar(bytes(scal[t]), k) + seed))
