@@ -56,6 +56,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
     return p.parse_args()
 
 
@@ -183,6 +184,23 @@ def reference_cpu(prefix: str, steps: int, warmup: int, step_seconds: float = 2.
             "ms_per_step": dt / steps * 1e3}
 
 
+def reference_cuda_kernel(b, lx, prefix: str) -> dict | None:
+    """The reference's own CUDA kernel (src/gpu/kernel.cu + common.h, BATCH 64,
+    block 128, SMs x 2048 threads as src/gpu/cuda.rs runs it) on this GPU, on
+    the same prefix, with seeded starts whose first public keys come from
+    lxmfv_first_public_keys."""
+    from oracle import oracle as O
+    if O.ref_cuda() is None:
+        return None
+    threads = O.ref_cuda().refcu_default_threads()
+    setup = lx.seeded_setup(SEED + 77, threads)
+    upc = b.first_public_keys(setup.scalars)
+    r = O.ref_cuda_walk(upc, 64, 1, 3, setup.ed_pub, lx.name_hash(), lx.prefix_parse(prefix))
+    return {"value": r["keys_per_s"], "unit": "keys/s", "threads": threads, "ms_per_launch": r["ms_per_launch"],
+            "sample": "3 timed launches of 64 batches of 64 keys per thread (CUDA events), after 1 warm-up",
+            "build": "reference src/gpu/kernel.cu + common.h, nvcc -gencode arch=compute_100a,code=sm_100a -O3"}
+
+
 def main() -> None:
     a = parse()
     world, rank, local = dist_setup()
@@ -307,6 +325,8 @@ def main() -> None:
     }
     if rank == 0 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prefix)
+    if rank == 0 and not a.no_ref_cuda:
+        line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)
     b.close()
     if world > 1:
         dist.destroy_process_group()

@@ -103,6 +103,13 @@ int lxmfv_init(lxmfv_handle* h, const uint32_t* u_prev_cur, size_t n_words);
  * CPU, followed by Backend::init. */
 int lxmfv_init_from_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t n_bytes);
 
+/* u(k-8) and u(k) for `count` start scalars (32 LE bytes each, clamped with
+ * room to step), computed on the GPU: 16 little-endian words per scalar into
+ * u_prev_cur, the layout lxmfv_init takes.  Replaces first_public_keys
+ * (mod.rs:212-228), which makes two X25519 per lane on the CPU.  Independent
+ * of the handle's lanes and walker state. */
+int lxmfv_first_public_keys(lxmfv_handle* h, const uint8_t* scalars, size_t count, uint32_t* u_prev_cur);
+
 /* Runs one launch of the walk and waits for it: every lane walks
  * args->iters * B keys from where it stopped.  Writes up to `hits_cap` hits
  * to `hits` and their total count (which may exceed hits_cap and
@@ -197,10 +204,12 @@ int lxmfv_fe_op(lxmfv_handle* h, int op, const uint32_t* a, const uint32_t* b, u
 int lxmfv_address_chain(lxmfv_handle* h, const uint8_t* pks, const uint8_t name_hash[10], uint8_t* out,
                         uint64_t count);
 
-/* Integer-pipe throughput probe: runs `kind` (0: IMAD, 1: IMAD.HI-class
- * mad.hi, 2: LOP3/IADD3/SHF mix) on every SM for about `ms` milliseconds and
- * returns lane-operations per second in *ops_per_s.  Diagnostic with no
- * counterpart in the reference: the denominator of the integer roofline. */
+/* Integer-pipe throughput probe: runs `kind` on every SM for about `ms`
+ * milliseconds and returns lane-operations per second in *ops_per_s.
+ * Kinds: 0 mad.lo.u32, 1 mad.hi.u32, 2 xor + funnel shift, 3 mad.wide.u32
+ * with a 64-bit addend, 4 add.u32, 5 mad.lo.u32 + xor (two pipes at once),
+ * 6 funnel shift, 7 xor.  Diagnostic with no counterpart in the reference:
+ * the denominators of the integer roofline. */
 int lxmfv_peak_probe(lxmfv_handle* h, int kind, float ms, double* ops_per_s);
 
 #ifdef __cplusplus

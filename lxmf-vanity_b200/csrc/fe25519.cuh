@@ -192,27 +192,45 @@ __device__ __forceinline__ fe fe_canon(const fe& a) {
     return o;
 }
 
-__device__ __forceinline__ fe fe_sqr_n(fe a, int n) {
-#pragma unroll 1
-    for (int i = 0; i < n; i++) a = fe_sqr(a);
-    return a;
-}
+// The ref10 addition chain for z^(p-2) (254 squarings, 11 multiplications;
+// the chain of the reference's fe_invert, common.h:115-128), as a table that
+// a loop walks, so that its code holds one square and one multiply instead of
+// 265 inlined bodies.  After z2 = z^2, step s squares the running value
+// kSq[s] times and multiplies it by operand kOp[s]; kSave[s] names the slot
+// that keeps the result for a later step.
+// Operands: 0 z, 1 z2, 2 z9, 3 z11, 4 z^(2^10-1), 5 z^(2^50-1), 6 the step's
+// own input (z^(2^5-1), z^(2^10-1), ... doubling the run of ones).
+__device__ __constant__ uint8_t kInvSq[11] = {2, 0, 1, 5, 10, 20, 10, 50, 100, 50, 5};
+__device__ __constant__ uint8_t kInvOp[11] = {0, 1, 2, 6, 6, 6, 4, 6, 6, 5, 3};
+__device__ __constant__ uint8_t kInvSave[11] = {2, 3, 0, 4, 0, 0, 5, 0, 0, 0, 0};
 
-// z^(p-2) by the ref10 addition chain (254 squarings, 11 multiplications),
-// the chain of the reference's fe_invert (common.h:115-128).  0 maps to 0.
+// z^(p-2).  0 maps to 0.
 __device__ __noinline__ fe fe_invert(fe z) {
     fe z2 = fe_sqr(z);
-    fe z9 = fe_mul(fe_sqr_n(z2, 2), z);
-    fe z11 = fe_mul(z9, z2);
-    fe z2_5_0 = fe_mul(fe_sqr(z11), z9);
-    fe z2_10_0 = fe_mul(fe_sqr_n(z2_5_0, 5), z2_5_0);
-    fe z2_20_0 = fe_mul(fe_sqr_n(z2_10_0, 10), z2_10_0);
-    fe z2_40_0 = fe_mul(fe_sqr_n(z2_20_0, 20), z2_20_0);
-    fe z2_50_0 = fe_mul(fe_sqr_n(z2_40_0, 10), z2_10_0);
-    fe z2_100_0 = fe_mul(fe_sqr_n(z2_50_0, 50), z2_50_0);
-    fe z2_200_0 = fe_mul(fe_sqr_n(z2_100_0, 100), z2_100_0);
-    fe z2_250_0 = fe_mul(fe_sqr_n(z2_200_0, 50), z2_50_0);
-    return fe_mul(fe_sqr_n(z2_250_0, 5), z11);
+    fe z9 = z, z11 = z, z10 = z, z50 = z;
+    fe t = z2;
+#pragma unroll 1
+    for (int s = 0; s < 11; s++) {
+        const fe base = t;
+        const int n = kInvSq[s];
+#pragma unroll 1
+        for (int i = 0; i < n; i++) t = fe_sqr(t);
+        const int op = kInvOp[s];
+        fe m = base;
+        m = (op == 0) ? z : m;
+        m = (op == 1) ? z2 : m;
+        m = (op == 2) ? z9 : m;
+        m = (op == 3) ? z11 : m;
+        m = (op == 4) ? z10 : m;
+        m = (op == 5) ? z50 : m;
+        t = fe_mul(t, m);
+        const int sv = kInvSave[s];
+        z9 = (sv == 2) ? t : z9;
+        z11 = (sv == 3) ? t : z11;
+        z10 = (sv == 4) ? t : z10;
+        z50 = (sv == 5) ? t : z50;
+    }
+    return t;
 }
 
 // Conditional swap by mask (m all ones or all zeros), without branches.

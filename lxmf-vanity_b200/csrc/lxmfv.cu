@@ -82,27 +82,10 @@ walk_fn pick_walk(uint32_t batch, uint32_t block) {
     return nullptr;
 }
 
-// SHA-256 rounds 0 and 1 of the destination block, which see only the name
-// hash: the same for every key of a search.
-void block3_head(const uint32_t nh[3], uint32_t head[8]) {
-    static const uint32_t K0 = 0x428a2f98u, K1 = 0x71374491u;
-    auto rotr = [](uint32_t x, int n) { return (x >> n) | (x << (32 - n)); };
-    uint32_t a = 0x6a09e667u, b = 0xbb67ae85u, c = 0x3c6ef372u, d = 0xa54ff53au;
-    uint32_t e = 0x510e527fu, f = 0x9b05688cu, g = 0x1f83d9abu, hh = 0x5be0cd19u;
-    const uint32_t kw[2] = {K0 + nh[0], K1 + nh[1]};
-    for (int i = 0; i < 2; i++) {
-        const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + kw[i];
-        const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
-        hh = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
-    }
-    head[0] = a; head[1] = b; head[2] = c; head[3] = d; head[4] = e; head[5] = f; head[6] = g; head[7] = hh;
-}
-
 void fill_addr_consts(lxsha::AddrConsts& ac, const uint32_t ed[8], const uint32_t nh[3], const uint32_t want[4],
                       const uint32_t mask[4]) {
     for (int i = 0; i < 8; i++) ac.ed[i] = ed ? ed[i] : 0;
     for (int i = 0; i < 3; i++) ac.nh[i] = nh[i];
-    block3_head(nh, ac.head);
     for (int i = 0; i < 4; i++) {
         ac.want[i] = want ? want[i] : 0;
         ac.mask[i] = mask ? mask[i] : 0;
@@ -141,6 +124,27 @@ int ensure_dump(lxmfv_handle* h, size_t keys) {
 
 int set_device(lxmfv_handle* h) {
     CU(h, cudaSetDevice(h->device));
+    return LXMFV_OK;
+}
+
+// u(8B), the fixed step point (mod.rs:111, main.rs:244), as 8 LE words.
+fe u8b() {
+    static const uint32_t U8B[8] = {0x48c99968u, 0xf1716fedu, 0xad74a91eu, 0x7a78edcau,
+                                    0xc8b65ca1u, 0xd83b884du, 0xaad65c2du, 0x275fa6d7u};
+    fe q;
+    for (int i = 0; i < 8; i++) q.v[i] = U8B[i];
+    return q;
+}
+
+int check_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t count) {
+    for (size_t t = 0; t < count; t++) {
+        const uint8_t* k = scalars + 32 * t;
+        if ((k[0] & 7) != 0 || (k[31] & 0xC0) != 0x40)
+            return fail(h, LXMFV_ERR_ARG, "scalar %zu is not clamped (k mod 8 = 0, bit 254 set, bit 255 clear)", t);
+        bool low_all_clear = k[31] == 64;
+        for (int i = 0; i < 31; i++) low_all_clear = low_all_clear && k[i] == 0;
+        if (low_all_clear) return fail(h, LXMFV_ERR_ARG, "scalar %zu is 2^254: k - 8 would not be clamped", t);
+    }
     return LXMFV_OK;
 }
 
@@ -242,28 +246,43 @@ int lxmfv_init_from_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t n_by
     if (n_bytes != (size_t)h->lanes * 32)
         return fail(h, LXMFV_ERR_ARG, "scalars have %zu bytes; %u lanes need %zu", n_bytes, h->lanes,
                     (size_t)h->lanes * 32);
-    for (size_t t = 0; t < h->lanes; t++) {
-        const uint8_t* k = scalars + 32 * t;
-        if ((k[0] & 7) != 0 || (k[31] & 0xC0) != 0x40)
-            return fail(h, LXMFV_ERR_ARG, "scalar %zu is not clamped (k mod 8 = 0, bit 254 set, bit 255 clear)", t);
-    }
+    if (int rc = check_scalars(h, scalars, h->lanes)) return rc;
     if (int rc = set_device(h)) return rc;
     uint32_t* d = nullptr;
     CU(h, cudaMalloc(&d, n_bytes));
     cudaError_t e = cudaMemcpyAsync(d, scalars, n_bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
-        fe q;
-        // u(8B), the fixed step point (mod.rs:111, main.rs:244).
-        static const uint32_t U8B[8] = {0x48c99968u, 0xf1716fedu, 0xad74a91eu, 0x7a78edcau,
-                                        0xc8b65ca1u, 0xd83b884du, 0xaad65c2du, 0x275fa6d7u};
-        for (int i = 0; i < 8; i++) q.v[i] = U8B[i];
-        lxk::ladder_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes, q);
+        lxk::ladder_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes, u8b());
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(d);
     if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "init_from_scalars: %s", cudaGetErrorString(e));
     h->initialised = true;
+    h->err.clear();
+    return LXMFV_OK;
+}
+
+int lxmfv_first_public_keys(lxmfv_handle* h, const uint8_t* scalars, size_t count, uint32_t* u_prev_cur) {
+    if (!h || !scalars || !u_prev_cur) return fail(h, LXMFV_ERR_ARG, "null argument");
+    if (!h->sms) return fail(h, LXMFV_ERR_STATE, "handle is not open");
+    if (count == 0) return LXMFV_OK;
+    if (count > (1u << 30)) return fail(h, LXMFV_ERR_ARG, "count %zu too large", count);
+    if (int rc = check_scalars(h, scalars, count)) return rc;
+    if (int rc = set_device(h)) return rc;
+    uint32_t *ds = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&ds, count * 32);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, count * 64);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, scalars, count * 32, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        lxk::first_keys_kernel<<<(unsigned)((count + 127) / 128), 128, 0, h->stream>>>(dout, ds, (uint32_t)count, u8b());
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u_prev_cur, dout, count * 64, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(ds);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "first_public_keys: %s", cudaGetErrorString(e));
     h->err.clear();
     return LXMFV_OK;
 }
@@ -428,12 +447,12 @@ int lxmfv_address_chain(lxmfv_handle* h, const uint8_t* pks, const uint8_t name_
 }
 
 int lxmfv_peak_probe(lxmfv_handle* h, int kind, float ms, double* ops_per_s) {
-    if (!h || !ops_per_s || kind < 0 || kind > 2) return fail(h, LXMFV_ERR_ARG, "bad argument");
+    if (!h || !ops_per_s || kind < 0 || kind > 7) return fail(h, LXMFV_ERR_ARG, "bad argument");
     if (int rc = set_device(h)) return rc;
     uint32_t* sink = nullptr;
     CU(h, cudaMalloc(&sink, sizeof(uint32_t)));
     const int blocks = h->sms * 8, threads = 256;
-    const double per_iter = (double)blocks * threads * 16 * 8 * (kind == 2 ? 2 : 1);
+    const double per_iter = (double)blocks * threads * 16 * 8 * ((kind == 2 || kind == 5) ? 2 : 1);
     uint32_t iters = 64;
     float t = 0;
     cudaError_t e = cudaSuccess;

@@ -3,13 +3,17 @@
 //   identity hash = SHA-256(u || ed)[0..16]          64-byte message: 2 blocks
 //   destination   = SHA-256(name_hash || ih)[0..16]  26-byte message: 1 block
 //
-// Same three compressions as the reference's lxmf_address (src/gpu/common.h:
-// 221-253) and the CPU path (src/main.rs:179-189), specialised:
-//   - block 2 is the fixed padding block of a 64-byte message, so its whole
-//     message schedule is a compile-time constant (folded into K + W);
-//   - block 3 carries the search's name hash in words 0-2 and zeros in words
-//     7-14, so rounds 0 and 1 (which see only the name hash) are done once per
-//     search on the host (sha_block3_head) and their zero words fold away;
+// The three compressions of the reference's lxmf_address (src/gpu/common.h:
+// 221-253) and of the CPU path (src/main.rs:179-189).  Code size matters as
+// much as instruction count here: the walk kernel keeps tens of warps per SM
+// in flight, and a fully unrolled chain (three times 64 rounds) does not fit
+// the instruction caches.  So:
+//   - rounds run as loops over 16-round unrolled bodies (the 8 working
+//     variables rotate statically inside a body, so no moves are needed);
+//   - blocks 1 and 3 share one generic compression (a two-pass loop);
+//   - block 2, the fixed padding block of a 64-byte message, has a constant
+//     message schedule: its rounds read precomputed K + W words (kKW2) and
+//     skip the schedule entirely;
 //   - only the first four output words are formed: the destination hash.
 #pragma once
 #include <cstdint>
@@ -26,6 +30,18 @@ __device__ __constant__ uint32_t K[64] = {
     0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
     0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
 
+// K[i] + W[i] for the padding block of a 64-byte message
+// (W = 0x80000000, 0 x 14, 512, extended by the FIPS 180-4 schedule).
+__device__ __constant__ uint32_t kKW2[64] = {
+    0xc28a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+    0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf374,
+    0x649b69c1, 0xf0fe4786, 0x0fe1edc6, 0x240cf254, 0x4fe9346f, 0x6cc984be, 0x61b9411e, 0x16f988fa,
+    0xf2c65152, 0xa88e5a6d, 0xb019fc65, 0xb9d99ec7, 0x9a1231c3, 0xe70eeaa0, 0xfdb1232b, 0xc7353eb0,
+    0x3069bad5, 0xcb976d5f, 0x5a0f118f, 0xdc1eeefd, 0x0a35b689, 0xde0b7a04, 0x58f4ca9d, 0xe15d5b16,
+    0x007f3e86, 0x37088980, 0xa507ea32, 0x6fab9537, 0x17406110, 0x0d8cd6f1, 0xcdaa3b6d, 0xc0bbbe37,
+    0x83613bda, 0xdb48a363, 0x0b02e931, 0x6fd15ca7, 0x521afaca, 0x31338431, 0x6ed41a95, 0x6d437890,
+    0xc39c91f2, 0x9eccabbd, 0xb5c9a0e6, 0x532fb63c, 0xd2c741c6, 0x07237ea3, 0xa4954b68, 0x4c191d76};
+
 __device__ __forceinline__ uint32_t rotr(uint32_t x, uint32_t n) { return __funnelshift_r(x, x, n); }
 __device__ __forceinline__ uint32_t bsig0(uint32_t a) { return rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22); }
 __device__ __forceinline__ uint32_t bsig1(uint32_t e) { return rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25); }
@@ -34,19 +50,70 @@ __device__ __forceinline__ uint32_t ssig1(uint32_t w) { return rotr(w, 17) ^ rot
 __device__ __forceinline__ uint32_t ch(uint32_t e, uint32_t f, uint32_t g) { return (e & f) ^ (~e & g); }
 __device__ __forceinline__ uint32_t maj(uint32_t a, uint32_t b, uint32_t c) { return (a & b) | (c & (a | b)); }
 
-// Rounds [R0, 64) of one compression over the 16 message words `w`
-// (overwritten by the rolling schedule), with the working state in s[0..7].
-// The caller adds the chaining value.
-template <int R0>
-__device__ __forceinline__ void rounds(uint32_t s[8], uint32_t w[16]) {
-    uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
-#pragma unroll
-    for (int i = R0; i < 64; i++) {
-        if (i >= 16) w[i & 15] += ssig0(w[(i - 15) & 15]) + w[(i - 7) & 15] + ssig1(w[(i - 2) & 15]);
-        const uint32_t t1 = h + bsig1(e) + ch(e, f, g) + K[i] + w[i & 15];
-        const uint32_t t2 = bsig0(a) + maj(a, b, c);
-        h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+// One round: the new e lands in d and the new a in h (the caller rotates names).
+#define LXSHA_R(a, b, c, d, e, f, g, h, kw)                          \
+    {                                                                \
+        const uint32_t t1_ = h + bsig1(e) + ch(e, f, g) + (kw);      \
+        d += t1_;                                                    \
+        h = t1_ + bsig0(a) + maj(a, b, c);                           \
     }
+
+#define LXSHA_SCHED(w, r) (w[(r)] += ssig0(w[((r) + 1) & 15]) + w[((r) + 9) & 15] + ssig1(w[((r) + 14) & 15]))
+
+// 16 rounds with message words (SCHED: extend the schedule in place first).
+template <bool SCHED>
+__device__ __forceinline__ void rounds16(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t& e,
+                                         uint32_t& f, uint32_t& g, uint32_t& h, uint32_t w[16], const uint32_t* k) {
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const int r = 8 * half;
+        if (SCHED) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) LXSHA_SCHED(w, r + i);
+        }
+        LXSHA_R(a, b, c, d, e, f, g, h, k[r + 0] + w[r + 0]);
+        LXSHA_R(h, a, b, c, d, e, f, g, k[r + 1] + w[r + 1]);
+        LXSHA_R(g, h, a, b, c, d, e, f, k[r + 2] + w[r + 2]);
+        LXSHA_R(f, g, h, a, b, c, d, e, k[r + 3] + w[r + 3]);
+        LXSHA_R(e, f, g, h, a, b, c, d, k[r + 4] + w[r + 4]);
+        LXSHA_R(d, e, f, g, h, a, b, c, k[r + 5] + w[r + 5]);
+        LXSHA_R(c, d, e, f, g, h, a, b, k[r + 6] + w[r + 6]);
+        LXSHA_R(b, c, d, e, f, g, h, a, k[r + 7] + w[r + 7]);
+    }
+}
+
+// 16 rounds whose K + W words are given (a constant message).
+__device__ __forceinline__ void rounds16_kw(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t& e,
+                                            uint32_t& f, uint32_t& g, uint32_t& h, const uint32_t* kw) {
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const int r = 8 * half;
+        LXSHA_R(a, b, c, d, e, f, g, h, kw[r + 0]);
+        LXSHA_R(h, a, b, c, d, e, f, g, kw[r + 1]);
+        LXSHA_R(g, h, a, b, c, d, e, f, kw[r + 2]);
+        LXSHA_R(f, g, h, a, b, c, d, e, kw[r + 3]);
+        LXSHA_R(e, f, g, h, a, b, c, d, kw[r + 4]);
+        LXSHA_R(d, e, f, g, h, a, b, c, kw[r + 5]);
+        LXSHA_R(c, d, e, f, g, h, a, b, kw[r + 6]);
+        LXSHA_R(b, c, d, e, f, g, h, a, kw[r + 7]);
+    }
+}
+
+// 64 rounds over message w (overwritten by the schedule); s in, working
+// state out (the caller adds the chaining value).
+__device__ __forceinline__ void compress(uint32_t s[8], uint32_t w[16]) {
+    uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
+    rounds16<false>(a, b, c, d, e, f, g, h, w, K);
+#pragma unroll 1
+    for (int j = 1; j < 4; j++) rounds16<true>(a, b, c, d, e, f, g, h, w, K + 16 * j);
+    s[0] = a; s[1] = b; s[2] = c; s[3] = d; s[4] = e; s[5] = f; s[6] = g; s[7] = h;
+}
+
+// 64 rounds of the constant padding block.
+__device__ __forceinline__ void compress_pad64(uint32_t s[8]) {
+    uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
+#pragma unroll 1
+    for (int j = 0; j < 4; j++) rounds16_kw(a, b, c, d, e, f, g, h, kKW2 + 16 * j);
     s[0] = a; s[1] = b; s[2] = c; s[3] = d; s[4] = e; s[5] = f; s[6] = g; s[7] = h;
 }
 
@@ -63,10 +130,14 @@ __device__ __forceinline__ void rounds(uint32_t s[8], uint32_t w[16]) {
 struct AddrConsts {
     uint32_t ed[8];     // Ed25519 public key, big-endian words (block-1 words 8..15)
     uint32_t nh[3];     // name hash, big-endian words; nh[2] holds bytes 8, 9 in its top half
-    uint32_t head[8];   // block-3 working state after rounds 0 and 1 (from IV, nh[0], nh[1])
     uint32_t want[4];   // prefix compare: (dest[k] & mask[k]) == want[k]
     uint32_t mask[4];
 };
+
+__device__ __forceinline__ void iv(uint32_t s[8]) {
+    s[0] = LXSHA_IV0; s[1] = LXSHA_IV1; s[2] = LXSHA_IV2; s[3] = LXSHA_IV3;
+    s[4] = LXSHA_IV4; s[5] = LXSHA_IV5; s[6] = LXSHA_IV6; s[7] = LXSHA_IV7;
+}
 
 // Destination hash (4 big-endian words) of a 64-byte public key whose first
 // 32 bytes are the little-endian words u[0..7] and whose last 32 bytes are
@@ -79,35 +150,32 @@ __device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi
     for (int i = 0; i < 8; i++) w[i] = __byte_perm(u[i], 0, 0x0123);
 #pragma unroll
     for (int i = 0; i < 8; i++) w[8 + i] = hi[i];
-    s[0] = LXSHA_IV0; s[1] = LXSHA_IV1; s[2] = LXSHA_IV2; s[3] = LXSHA_IV3;
-    s[4] = LXSHA_IV4; s[5] = LXSHA_IV5; s[6] = LXSHA_IV6; s[7] = LXSHA_IV7;
-    rounds<0>(s, w);
-    uint32_t h1[8];
-    h1[0] = s[0] + LXSHA_IV0; h1[1] = s[1] + LXSHA_IV1; h1[2] = s[2] + LXSHA_IV2; h1[3] = s[3] + LXSHA_IV3;
-    h1[4] = s[4] + LXSHA_IV4; h1[5] = s[5] + LXSHA_IV5; h1[6] = s[6] + LXSHA_IV6; h1[7] = s[7] + LXSHA_IV7;
-    // Block 2: the padding block of a 64-byte message (constant schedule).
-    w[0] = 0x80000000u;
+    iv(s);
+#pragma unroll 1
+    for (int pass = 0;; pass++) {
+        compress(s, w);
+        if (pass == 1) break;
+        // Block 2: the padding block, chained from block 1.
+        uint32_t h1[8], t[8];
+        h1[0] = s[0] + LXSHA_IV0; h1[1] = s[1] + LXSHA_IV1; h1[2] = s[2] + LXSHA_IV2; h1[3] = s[3] + LXSHA_IV3;
+        h1[4] = s[4] + LXSHA_IV4; h1[5] = s[5] + LXSHA_IV5; h1[6] = s[6] + LXSHA_IV6; h1[7] = s[7] + LXSHA_IV7;
 #pragma unroll
-    for (int i = 1; i < 15; i++) w[i] = 0;
-    w[15] = 512;
+        for (int i = 0; i < 8; i++) t[i] = h1[i];
+        compress_pad64(t);
+        const uint32_t ih0 = t[0] + h1[0], ih1 = t[1] + h1[1], ih2 = t[2] + h1[2], ih3 = t[3] + h1[3];
+        // Block 3: name_hash (10) || identity hash (16) || padding, 208 bits.
+        w[0] = c.nh[0];
+        w[1] = c.nh[1];
+        w[2] = c.nh[2] | (ih0 >> 16);
+        w[3] = __funnelshift_l(ih1, ih0, 16);
+        w[4] = __funnelshift_l(ih2, ih1, 16);
+        w[5] = __funnelshift_l(ih3, ih2, 16);
+        w[6] = (ih3 << 16) | 0x8000u;
 #pragma unroll
-    for (int i = 0; i < 8; i++) s[i] = h1[i];
-    rounds<0>(s, w);
-    const uint32_t ih0 = s[0] + h1[0], ih1 = s[1] + h1[1], ih2 = s[2] + h1[2], ih3 = s[3] + h1[3];
-    // Block 3: name_hash (10) || identity hash (16) || padding, length 208 bits.
-    w[0] = c.nh[0];
-    w[1] = c.nh[1];
-    w[2] = c.nh[2] | (ih0 >> 16);
-    w[3] = __funnelshift_l(ih1, ih0, 16);
-    w[4] = __funnelshift_l(ih2, ih1, 16);
-    w[5] = __funnelshift_l(ih3, ih2, 16);
-    w[6] = (ih3 << 16) | 0x8000u;
-#pragma unroll
-    for (int i = 7; i < 15; i++) w[i] = 0;
-    w[15] = 26 * 8;
-#pragma unroll
-    for (int i = 0; i < 8; i++) s[i] = c.head[i];
-    rounds<2>(s, w);
+        for (int i = 7; i < 15; i++) w[i] = 0;
+        w[15] = 26 * 8;
+        iv(s);
+    }
     out[0] = s[0] + LXSHA_IV0;
     out[1] = s[1] + LXSHA_IV1;
     out[2] = s[2] + LXSHA_IV2;

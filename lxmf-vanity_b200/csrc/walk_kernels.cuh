@@ -163,10 +163,8 @@ __global__ void init_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __res
 // (X3:Z3) = (s+1) Q = k B: exactly the walk's (P(n-1), P(n)) at n = 0, left
 // projective.  The ladder step is RFC 7748's, with a24 = 121665 and swaps by
 // masks (no branch on a secret bit).
-__global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ scalars,
-                                                     uint32_t lanes, fe q) {
-    const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lane >= lanes) return;
+__device__ __forceinline__ void ladder_pair(const uint32_t* __restrict__ scalars, uint32_t lane, const fe& q, fe& x2,
+                                            fe& z2, fe& x3, fe& z3) {
     uint32_t k[8], s[8];
 #pragma unroll
     for (int w = 0; w < 8; w++) k[w] = scalars[(size_t)lane * 8 + w];
@@ -181,7 +179,10 @@ __global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* 
         s[w] = x - borrow;
         borrow = (x < borrow) ? 1u : 0u;
     }
-    fe x2 = fe_one(), z2 = fe_zero(), x3 = q, z3 = fe_one();
+    x2 = fe_one();
+    z2 = fe_zero();
+    x3 = q;
+    z3 = fe_one();
     uint32_t swap = 0;
 #pragma unroll 1
     for (int t = 251; t >= 0; --t) {
@@ -202,11 +203,38 @@ __global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* 
     }
     fe_cswap(x2, x3, 0u - swap);
     fe_cswap(z2, z3, 0u - swap);
+}
+
+__global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ scalars,
+                                                     uint32_t lanes, fe q) {
+    const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lane >= lanes) return;
+    fe x2, z2, x3, z3;
+    ladder_pair(scalars, lane, q, x2, z2, x3, z3);
     store_fe(state, 0, lane, lanes, x2);
     store_fe(state, 1, lane, lanes, z2);
     store_fe(state, 2, lane, lanes, x3);
     store_fe(state, 3, lane, lanes, z3);
     ns[lane] = 0;
+}
+
+// first_public_keys (mod.rs:212-228) on the GPU: u(k-8) and u(k) as 16
+// canonical little-endian words per lane, the input of Backend::init.  One
+// inversion of Z2 * Z3 serves both coordinates.
+__global__ void __launch_bounds__(128) first_keys_kernel(uint32_t* __restrict__ upc, const uint32_t* __restrict__ scalars,
+                                                         uint32_t lanes, fe q) {
+    const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lane >= lanes) return;
+    fe x2, z2, x3, z3;
+    ladder_pair(scalars, lane, q, x2, z2, x3, z3);
+    const fe inv = fe_invert(fe_mul(z2, z3));
+    const fe u_prev = fe_canon(fe_mul(x2, fe_mul(inv, z3)));
+    const fe u_cur = fe_canon(fe_mul(x3, fe_mul(inv, z2)));
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+        upc[(size_t)lane * 16 + w] = u_prev.v[w];
+        upc[(size_t)lane * 16 + 8 + w] = u_cur.v[w];
+    }
 }
 
 // ---- Primitive kernels for the field / hash microbench.
@@ -217,6 +245,16 @@ __device__ __forceinline__ fe load_words_drop255(const uint32_t* p) {
     const uint4 lo = p4[0], hi = p4[1];
     r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = lo.z; r.v[3] = lo.w;
     r.v[4] = hi.x; r.v[5] = hi.y; r.v[6] = hi.z; r.v[7] = hi.w & 0x7fffffffu;
+    return r;
+}
+
+// All 256 bits: an intermediate value of the 8-word representation.
+__device__ __forceinline__ fe load_words(const uint32_t* p) {
+    fe r;
+    const uint4* p4 = reinterpret_cast<const uint4*>(p);
+    const uint4 lo = p4[0], hi = p4[1];
+    r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = lo.z; r.v[3] = lo.w;
+    r.v[4] = hi.x; r.v[5] = hi.y; r.v[6] = hi.z; r.v[7] = hi.w;
     return r;
 }
 
@@ -254,7 +292,7 @@ __global__ void fe_batch_invert_kernel(const uint32_t* __restrict__ a, uint32_t*
         }
         fe inv = fe_invert(acc);
         for (int i = (int)len - 1; i >= 0; i--) {
-            const fe pre = load_words_drop255(out + 8 * (base + i));
+            const fe pre = load_words(out + 8 * (base + i));
             store_words(out + 8 * (base + i), fe_canon(fe_mul(inv, pre)));
             inv = fe_mul(inv, load_words_drop255(a + 8 * (base + i)));
         }
@@ -282,46 +320,47 @@ __global__ void address_chain_kernel(const uint32_t* __restrict__ pk, lxsha::Add
 // Each thread runs 8 independent dependency chains of one instruction class
 // so that issue, not latency, is the limit; `sink` keeps the work alive.
 
+// Operations counted per step and chain: kinds 2 and 5 issue two.
+//   0 mad.lo.u32   1 mad.hi.u32   2 xor + shf   3 mad.wide.u32 (64-bit addend)
+//   4 add.u32      5 mad.lo + xor (two pipes)   6 shf only   7 xor only
 __global__ void __launch_bounds__(256) probe_kernel(int kind, uint32_t iters, uint32_t seed, uint32_t* sink) {
-    uint32_t x[8];
+    uint32_t x[8], y[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) x[j] = seed + threadIdx.x * 8 + j;
-    const uint32_t m = seed | 1u, c = seed ^ 0x9e3779b9u;
-    if (kind == 0) {
-#pragma unroll 1
-        for (uint32_t i = 0; i < iters; i++) {
-#pragma unroll
-            for (int r = 0; r < 16; r++) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(m), "r"(c));
-            }
-        }
-    } else if (kind == 1) {
-#pragma unroll 1
-        for (uint32_t i = 0; i < iters; i++) {
-#pragma unroll
-            for (int r = 0; r < 16; r++) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(m), "r"(c));
-            }
-        }
-    } else {
-#pragma unroll 1
-        for (uint32_t i = 0; i < iters; i++) {
-#pragma unroll
-            for (int r = 0; r < 16; r++) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    // one LOP3-class xor and one funnel shift per step
-                    asm volatile("xor.b32 %0, %0, %1;" : "+r"(x[j]) : "r"(c));
-                    asm volatile("shf.r.wrap.b32 %0, %0, %0, 7;" : "+r"(x[j]));
-                }
-            }
-        }
+    for (int j = 0; j < 8; j++) {
+        x[j] = seed + threadIdx.x * 8 + j;
+        y[j] = x[j] ^ 0x55555555u;
     }
+    const uint32_t m = seed | 1u, c = seed ^ 0x9e3779b9u;
+#define LXK_PROBE(BODY)                                   \
+    _Pragma("unroll 1") for (uint32_t i = 0; i < iters; i++) { \
+        _Pragma("unroll") for (int r = 0; r < 16; r++) {   \
+            _Pragma("unroll") for (int j = 0; j < 8; j++) { BODY; } \
+        }                                                  \
+    }
+    switch (kind) {
+        case 0: LXK_PROBE(asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(m), "r"(c))) break;
+        case 1: LXK_PROBE(asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(m), "r"(c))) break;
+        case 2:
+            LXK_PROBE(asm volatile("xor.b32 %0, %0, %1;" : "+r"(x[j]) : "r"(c));
+                      asm volatile("shf.r.wrap.b32 %0, %0, %0, 7;" : "+r"(x[j])))
+            break;
+        case 3:
+            LXK_PROBE(asm volatile("{.reg .u64 t; mov.b64 t, {%0, %1}; mad.wide.u32 t, %0, %2, t; mov.b64 {%0, %1}, t;}"
+                                   : "+r"(x[j]), "+r"(y[j]) : "r"(m)))
+            break;
+        // The neighbour operand keeps ptxas from folding repeated ops on one constant.
+        case 4: LXK_PROBE(asm volatile("add.u32 %0, %0, %1;" : "+r"(x[j]) : "r"(x[(j + 1) & 7]))) break;
+        case 5:
+            LXK_PROBE(asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(m), "r"(c));
+                      asm volatile("xor.b32 %0, %0, %1;" : "+r"(y[j]) : "r"(y[(j + 1) & 7])))
+            break;
+        case 6: LXK_PROBE(asm volatile("shf.r.wrap.b32 %0, %0, %0, 7;" : "+r"(x[j]))) break;
+        default: LXK_PROBE(asm volatile("xor.b32 %0, %0, %1;" : "+r"(x[j]) : "r"(x[(j + 1) & 7]))) break;
+    }
+#undef LXK_PROBE
     uint32_t acc = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc ^= x[j];
+    for (int j = 0; j < 8; j++) acc ^= x[j] ^ y[j];
     if (acc == 0x12345678u) sink[0] = acc;
 }
 

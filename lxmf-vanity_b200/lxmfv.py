@@ -67,6 +67,7 @@ SIGNATURES = {
     "lxmfv_batch": ([C.c_void_p], C.c_uint64),
     "lxmfv_init": ([C.c_void_p, _u32p, C.c_size_t], C.c_int),
     "lxmfv_init_from_scalars": ([C.c_void_p, _u8p, C.c_size_t], C.c_int),
+    "lxmfv_first_public_keys": ([C.c_void_p, _u8p, C.c_size_t, _u32p], C.c_int),
     "lxmfv_launch": ([C.c_void_p, C.POINTER(LaunchArgs), C.POINTER(Hit), C.c_uint32, _u32p, _u32p, _u32p], C.c_int),
     "lxmfv_launch_async": ([C.c_void_p, C.POINTER(LaunchArgs)], C.c_int),
     "lxmfv_collect": ([C.c_void_p, C.POINTER(Hit), C.c_uint32, _u32p, _u32p, _u32p], C.c_int),
@@ -297,6 +298,14 @@ class Backend:
         a = np.frombuffer(scalars, np.uint8) if isinstance(scalars, (bytes, bytearray)) else \
             np.ascontiguousarray(scalars, np.uint8).reshape(-1)
         self._check(lib().lxmfv_init_from_scalars(self._h, a.ctypes.data_as(_u8p), a.size))
+
+    def first_public_keys(self, scalars: np.ndarray) -> np.ndarray:
+        """u(k-8), u(k) per scalar on the GPU: (count, 16) LE words for init()."""
+        s = np.ascontiguousarray(scalars, np.uint8).reshape(-1, 32)
+        out = np.zeros((s.shape[0], 16), np.uint32)
+        self._check(lib().lxmfv_first_public_keys(self._h, s.ctypes.data_as(_u8p), s.shape[0],
+                                                  out.ctypes.data_as(_u32p)))
+        return out
 
     def launch(self, args: LaunchArgs, hits_cap: int | None = None, want_dump: bool = False,
                want_dump_addr: bool = False) -> tuple[list[tuple[int, int]], np.ndarray | None, np.ndarray | None, int]:

@@ -98,6 +98,51 @@ def ref():
     return _ref
 
 
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libref_cuda.so")
+_ref_cuda = None
+
+
+def ref_cuda():
+    """The reference's own CUDA kernel built for sm_100a (None when absent)."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        if not os.path.exists(REF_CUDA_SO):
+            return None
+        L = C.CDLL(REF_CUDA_SO)
+        L.refcu_walk.argtypes = [_u32p, C.c_uint32, C.c_uint32, C.c_int, C.c_int, _u32p, C.c_uint32, C.c_uint32,
+                                 C.c_uint32, _u32p, _u32p, _u32p, C.POINTER(C.c_double), C.POINTER(C.c_float), _u32p,
+                                 _u64p, C.c_uint32, _u32p]
+        L.refcu_walk.restype = C.c_int
+        L.refcu_default_threads.restype = C.c_int
+        _ref_cuda = L
+    return _ref_cuda
+
+
+def ref_cuda_walk(u_prev_cur: np.ndarray, iters: int, warmup: int, steps: int, ed_pub: bytes, nh: bytes,
+                  prefix: tuple[bytes, int], dump_threads: int = 0) -> dict:
+    """Runs the reference's walk kernel on the GPU; keys/s, hits, dump."""
+    L = ref_cuda()
+    upc = np.ascontiguousarray(u_prev_cur, np.uint32).reshape(-1, 16)
+    threads = upc.shape[0]
+    ed = np.frombuffer(ed_pub, ">u4").astype(np.uint32)
+    nhw = [int.from_bytes(nh[0:4], "big"), int.from_bytes(nh[4:8], "big"), (nh[8] << 24) | (nh[9] << 16)]
+    w, m = prefix_words(prefix)
+    want, mask = np.array(w, np.uint32), np.array(m, np.uint32)
+    q = np.frombuffer(u8b(), "<u4").astype(np.uint32)
+    rate, ms, n = C.c_double(0), C.c_float(0), C.c_uint32(0)
+    hits = np.zeros(2 * 4096, np.uint64)
+    dump = np.zeros(max(dump_threads, 1) * 64 * 8, np.uint32)
+    rc = L.refcu_walk(_p(upc, _u32p), threads, iters, warmup, steps, _p(ed, _u32p), nhw[0], nhw[1], nhw[2],
+                      _p(want, _u32p), _p(mask, _u32p), _p(q, _u32p), C.byref(rate), C.byref(ms), C.byref(n),
+                      _p(hits, _u64p), dump_threads, _p(dump, _u32p))
+    if rc != 0:
+        raise RuntimeError(f"reference CUDA kernel: CUDA error {rc}")
+    k = min(n.value, 4096)
+    return {"keys_per_s": rate.value, "ms_per_launch": ms.value, "n_hits": n.value,
+            "hits": [(int(hits[2 * i]), int(hits[2 * i + 1])) for i in range(k)],
+            "dump": dump[: dump_threads * 64 * 8] if dump_threads else None, "threads": threads}
+
+
 def _buf(b: bytes | bytearray | np.ndarray):
     if isinstance(b, np.ndarray):
         return b.ctypes.data_as(_u8p)

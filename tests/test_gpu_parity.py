@@ -101,6 +101,34 @@ def test_ladder_start_points_and_first_batch(backend, lx, oracle):
             assert bytes(hashes[t, i]) == oracle.lxmf_address(nh, bytes(keys[t, i]), setup.ed_pub)
 
 
+def test_first_public_keys_match_x25519(backend, lx, oracle):
+    """first_public_keys on the GPU: u(k-8), u(k) against plain X25519."""
+    setup = lx.seeded_setup(111, 300)
+    upc = backend.first_public_keys(setup.scalars)
+    for t in range(0, 300, 7):
+        k = bytes(setup.scalars[t])
+        assert upc[t, :8].tobytes() == oracle.x25519_base(oracle.previous_scalar(k)), t
+        assert upc[t, 8:].tobytes() == oracle.x25519_base(k), t
+    with pytest.raises(lx.LxmfvError):
+        backend.first_public_keys(np.zeros((2, 32), np.uint8))  # not clamped
+
+
+def test_reference_cuda_kernel_agrees(backend, lx, oracle):
+    """The reference's own walk kernel, built for sm_100a, and this one give
+    the same hits and public keys for the same lanes."""
+    if oracle.ref_cuda() is None:
+        pytest.skip("oracle/_ref/libref_cuda.so not built (needs the reference tree)")
+    lanes = backend.threads()
+    setup = lx.seeded_setup(121, lanes)
+    upc = backend.first_public_keys(setup.scalars)
+    pfx = lx.prefix_parse("b00")
+    r = oracle.ref_cuda_walk(upc, 4, 0, 1, setup.ed_pub, lx.name_hash(), pfx, dump_threads=8)
+    backend.init(upc)
+    hits, dump, _, n = _walk(backend, lx, setup, "b00", 4, dump_lanes=8)
+    assert r["n_hits"] == n and sorted(r["hits"]) == sorted(hits) and n > 100
+    assert (r["dump"] == dump).all()
+
+
 def test_reference_init_interface(backend, lx, oracle):
     """Backend::init from u(k-8), u(k) words gives the same walk as the ladder."""
     lanes = backend.threads()
