@@ -40,14 +40,24 @@ extern "C" {
 
 typedef struct lxmfv_handle lxmfv_handle;
 
+/* Walks.  Both visit the same keys k + 8n and give the same hashes and hits.
+ * GROUP: affine additions of table points i*8B to a centre point, one batch
+ *        inversion per group of `batch` keys (about half the field work).
+ * XADD:  the reference's x-only differential addition (common.h:316-325)
+ *        with Montgomery's batch inversion over `batch` keys. */
+#define LXMFV_WALK_GROUP 0
+#define LXMFV_WALK_XADD 1
+#define LXMFV_MAX_HALF_GROUP 128
+
 /* Opening options; zero fields take defaults.
  * Replaces the constants of src/gpu/cuda.rs:13-16 (BATCH, BLOCK,
  * THREADS_PER_SM) and CudaContext::new(0) (cuda.rs:33-64). */
 typedef struct {
     int32_t device;       /* CUDA device ordinal */
     uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
-    uint32_t batch;       /* keys per batch inversion B: 16, 32, 64 or 128; 0: 64 */
+    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32, 64, 128, 256; 0: 64 */
     uint32_t block;       /* threads per block: 128 or 256; 0: 256 */
+    uint32_t walk;        /* LXMFV_WALK_GROUP (0, default) or LXMFV_WALK_XADD */
     void* stream;         /* cudaStream_t to launch on; NULL: a stream of the handle's own */
 } lxmfv_options;
 
@@ -89,6 +99,10 @@ uint32_t lxmfv_threads(const lxmfv_handle* h);
 
 /* Keys per batch inversion: Backend::batch (mod.rs:46). */
 uint64_t lxmfv_batch(const lxmfv_handle* h);
+
+/* The handle's walk (LXMFV_WALK_GROUP or LXMFV_WALK_XADD).  No counterpart in
+ * the reference, which has the x-only walk only. */
+uint32_t lxmfv_walk(const lxmfv_handle* h);
 
 /* Sets every lane from u(k-8) and u(k): 16 little-endian words per lane,
  * n_words = 16 * lanes.  Walk indices restart at 0.  Replaces Backend::init

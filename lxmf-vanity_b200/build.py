@@ -27,7 +27,7 @@ CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra"]
 
 CU_SOURCES = ["lxmfv.cu"]
 CXX_SOURCES = ["host.cpp"]
-HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh"]
+HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "prim_kernels.cuh"]
 
 
 def _run(cmd: list[str], verbose: bool) -> str:

@@ -16,6 +16,8 @@
 #include <string>
 
 #include "../../include/lxmfv.h"
+#include "group_kernels.cuh"
+#include "prim_kernels.cuh"
 #include "walk_kernels.cuh"
 
 struct lxmfv_handle {
@@ -25,8 +27,9 @@ struct lxmfv_handle {
     std::string name;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    uint32_t walk = LXMFV_WALK_GROUP;
     uint32_t lanes = 0;
-    uint32_t batch = 64;
+    uint32_t batch = 64;  // keys per inversion: B (x-only walk) or G = 2M (grouped walk)
     uint32_t block = 256;
     uint32_t* d_state = nullptr;
     uint64_t* d_ns = nullptr;
@@ -41,6 +44,7 @@ struct lxmfv_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     bool initialised = false;
+    fe tu[LXMFV_MAX_HALF_GROUP + 1], tv[LXMFV_MAX_HALF_GROUP + 1];  // grouped walk: J, 1Q .. MQ
     std::string err;
 };
 
@@ -64,22 +68,77 @@ int fail(lxmfv_handle* h, int code, const char* fmt, ...) {
                         __FILE__, __LINE__);                                                 \
     } while (0)
 
-typedef void (*walk_fn)(lxk::WalkArgs);
+constexpr int minb(int block) { return block == 256 ? 2 : 4; }
 
-template <int B, int BLOCK>
-walk_fn walk_for() {
-    return lxk::walk_kernel<B, BLOCK, (BLOCK == 256 ? 2 : 4)>;
+// The walk kernel of a configuration, for the occupancy query.
+const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block) {
+#define LXMFV_X(B)                                                                                   \
+    if (batch == B)                                                                                  \
+        return block == 128 ? (const void*)lxk::walk_kernel<B, 128, minb(128)>                       \
+                            : (const void*)lxk::walk_kernel<B, 256, minb(256)>;
+#define LXMFV_G(G)                                                                                   \
+    if (batch == G)                                                                                  \
+        return block == 128 ? (const void*)lxk::group_walk_kernel<G / 2, 128, minb(128)>             \
+                            : (const void*)lxk::group_walk_kernel<G / 2, 256, minb(256)>;
+    if (block != 128 && block != 256) return nullptr;
+    if (walk == LXMFV_WALK_XADD) {
+        LXMFV_X(16) LXMFV_X(32) LXMFV_X(64) LXMFV_X(128)
+    } else if (walk == LXMFV_WALK_GROUP) {
+        LXMFV_G(32) LXMFV_G(64) LXMFV_G(128) LXMFV_G(256)
+    }
+#undef LXMFV_X
+#undef LXMFV_G
+    return nullptr;
 }
 
-walk_fn pick_walk(uint32_t batch, uint32_t block) {
-#define LXMFV_CASE(B)                                                 \
-    if (batch == B) return block == 128 ? walk_for<B, 128>() : walk_for<B, 256>();
-    LXMFV_CASE(16)
-    LXMFV_CASE(32)
-    LXMFV_CASE(64)
-    LXMFV_CASE(128)
-#undef LXMFV_CASE
-    return nullptr;
+template <int B>
+void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
+    const unsigned grid = (h->lanes + h->block - 1) / h->block;
+    if (h->block == 128) lxk::walk_kernel<B, 128, minb(128)><<<grid, 128, 0, h->stream>>>(wa);
+    else lxk::walk_kernel<B, 256, minb(256)><<<grid, 256, 0, h->stream>>>(wa);
+}
+
+template <int M>
+void launch_group(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
+    lxk::GroupArgs<M> ga;
+    ga.state = h->d_state;
+    ga.ns = h->d_ns;
+    ga.lanes = h->lanes;
+    ga.iters = iters;
+    ga.em = em;
+    for (int i = 0; i <= M; i++) {
+        ga.t.u[i] = h->tu[i];
+        ga.t.v[i] = h->tv[i];
+    }
+    const unsigned grid = (h->lanes + h->block - 1) / h->block;
+    if (h->block == 128) lxk::group_walk_kernel<M, 128, minb(128)><<<grid, 128, 0, h->stream>>>(ga);
+    else lxk::group_walk_kernel<M, 256, minb(256)><<<grid, 256, 0, h->stream>>>(ga);
+}
+
+void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const fe& q) {
+    if (h->walk == LXMFV_WALK_XADD) {
+        lxk::WalkArgs wa;
+        memset(&wa, 0, sizeof wa);
+        wa.state = h->d_state;
+        wa.ns = h->d_ns;
+        wa.lanes = h->lanes;
+        wa.iters = iters;
+        wa.q = q;
+        wa.em = em;
+        switch (h->batch) {
+            case 16: launch_xadd<16>(h, wa); break;
+            case 32: launch_xadd<32>(h, wa); break;
+            case 64: launch_xadd<64>(h, wa); break;
+            default: launch_xadd<128>(h, wa); break;
+        }
+    } else {
+        switch (h->batch) {
+            case 32: launch_group<16>(h, em, iters); break;
+            case 64: launch_group<32>(h, em, iters); break;
+            case 128: launch_group<64>(h, em, iters); break;
+            default: launch_group<128>(h, em, iters); break;
+        }
+    }
 }
 
 void fill_addr_consts(lxsha::AddrConsts& ac, const uint32_t ed[8], const uint32_t nh[3], const uint32_t want[4],
@@ -127,13 +186,31 @@ int set_device(lxmfv_handle* h) {
     return LXMFV_OK;
 }
 
+fe words8(const uint32_t w[8]) {
+    fe x;
+    for (int i = 0; i < 8; i++) x.v[i] = w[i];
+    return x;
+}
+
 // u(8B), the fixed step point (mod.rs:111, main.rs:244), as 8 LE words.
 fe u8b() {
     static const uint32_t U8B[8] = {0x48c99968u, 0xf1716fedu, 0xad74a91eu, 0x7a78edcau,
                                     0xc8b65ca1u, 0xd83b884du, 0xaad65c2du, 0x275fa6d7u};
-    fe q;
-    for (int i = 0; i < 8; i++) q.v[i] = U8B[i];
-    return q;
+    return words8(U8B);
+}
+
+// v(8B): the even square root of u^3 + A u^2 + u at u = u(8B); the grouped
+// walk's points are all multiples of this Q.  And its negation, p - v.
+fe v8b() {
+    static const uint32_t V[8] = {0x9f728718u, 0xc5296d6eu, 0x70c591f9u, 0x4f479c67u,
+                                  0x4066b08cu, 0x8dcf4469u, 0x8fb939e4u, 0x6085bbbau};
+    return words8(V);
+}
+
+fe v8b_neg() {
+    static const uint32_t V[8] = {0x608d78d5u, 0x3ad69291u, 0x8f3a6e06u, 0xb0b86398u,
+                                  0xbf994f73u, 0x7230bb96u, 0x7046c61bu, 0x1f7a4445u};
+    return words8(V);
 }
 
 int check_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t count) {
@@ -145,6 +222,26 @@ int check_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t count) {
         for (int i = 0; i < 31; i++) low_all_clear = low_all_clear && k[i] == 0;
         if (low_all_clear) return fail(h, LXMFV_ERR_ARG, "scalar %zu is 2^254: k - 8 would not be clamped", t);
     }
+    return LXMFV_OK;
+}
+
+// The grouped walk's table, computed once on the device and kept on the host
+// to travel in every launch's parameter block.
+int build_group_table(lxmfv_handle* h) {
+    const uint32_t m = h->batch / 2;
+    fe *du = nullptr, *dv = nullptr;
+    cudaError_t e = cudaMalloc(&du, sizeof(fe) * (m + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dv, sizeof(fe) * (m + 1));
+    if (e == cudaSuccess) {
+        lxk::group_table_kernel<<<1, ((m + 1 + 31) / 32) * 32, 0, h->stream>>>(du, dv, m, u8b(), v8b());
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->tu, du, sizeof(fe) * (m + 1), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->tv, dv, sizeof(fe) * (m + 1), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(du);
+    cudaFree(dv);
+    if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "group table: %s", cudaGetErrorString(e));
     return LXMFV_OK;
 }
 
@@ -161,10 +258,15 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     lxmfv_options o{};
     if (opts) o = *opts;
     h->device = o.device;
+    h->walk = o.walk;
     h->batch = o.batch ? o.batch : 64;
     h->block = o.block ? o.block : 256;
-    if (!pick_walk(h->batch, h->block) || (h->block != 128 && h->block != 256))
-        return fail(h, LXMFV_ERR_ARG, "unsupported batch %u / block %u (batch 16, 32, 64, 128; block 128, 256)",
+    if (h->walk != LXMFV_WALK_GROUP && h->walk != LXMFV_WALK_XADD)
+        return fail(h, LXMFV_ERR_ARG, "walk %u: 0 grouped, 1 x-only", h->walk);
+    if (!walk_kernel_ptr(h->walk, h->batch, h->block))
+        return fail(h, LXMFV_ERR_ARG,
+                    "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: 32, 64, "
+                    "128, 256; block 128 or 256)",
                     h->batch, h->block);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -190,9 +292,9 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     }
     CU(h, cudaEventCreate(&h->ev0));
     CU(h, cudaEventCreate(&h->ev1));
-    walk_fn fn = pick_walk(h->batch, h->block);
     int per_sm = 0;
-    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)h->block, 0));
+    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block),
+                                                        (int)h->block, 0));
     if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
     h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;
     CU(h, cudaMalloc(&h->d_state, (size_t)h->lanes * 32 * sizeof(uint32_t)));
@@ -202,6 +304,8 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     CU(h, cudaMemsetAsync(h->d_state, 0, (size_t)h->lanes * 32 * sizeof(uint32_t), h->stream));
     CU(h, cudaMemsetAsync(h->d_ns, 0, (size_t)h->lanes * sizeof(uint64_t), h->stream));
     if (int rc = ensure_hits(h, 4096)) return rc;
+    if (h->walk == LXMFV_WALK_GROUP)
+        if (int rc = build_group_table(h)) return rc;
     CU(h, cudaStreamSynchronize(h->stream));
     h->err.clear();
     return LXMFV_OK;
@@ -218,6 +322,8 @@ uint32_t lxmfv_threads(const lxmfv_handle* h) { return h ? h->lanes : 0; }
 
 uint64_t lxmfv_batch(const lxmfv_handle* h) { return h ? h->batch : 0; }
 
+uint32_t lxmfv_walk(const lxmfv_handle* h) { return h ? h->walk : 0; }
+
 int lxmfv_init(lxmfv_handle* h, const uint32_t* u_prev_cur, size_t n_words) {
     if (!h || !u_prev_cur) return fail(h, LXMFV_ERR_ARG, "null argument");
     if (!h->d_state) return fail(h, LXMFV_ERR_STATE, "handle is not open");
@@ -229,7 +335,13 @@ int lxmfv_init(lxmfv_handle* h, const uint32_t* u_prev_cur, size_t n_words) {
     CU(h, cudaMalloc(&d, n_words * sizeof(uint32_t)));
     cudaError_t e = cudaMemcpyAsync(d, u_prev_cur, n_words * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
-        lxk::init_kernel<<<(h->lanes + 255) / 256, 256, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes);
+        if (h->walk == LXMFV_WALK_XADD) {
+            lxk::init_kernel<<<(h->lanes + 255) / 256, 256, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes);
+        } else {
+            const uint32_t m = h->batch / 2;
+            lxk::group_init_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes,
+                                                                                   u8b(), v8b_neg(), h->tu[m], h->tv[m]);
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -252,7 +364,12 @@ int lxmfv_init_from_scalars(lxmfv_handle* h, const uint8_t* scalars, size_t n_by
     CU(h, cudaMalloc(&d, n_bytes));
     cudaError_t e = cudaMemcpyAsync(d, scalars, n_bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
-        lxk::ladder_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes, u8b());
+        if (h->walk == LXMFV_WALK_XADD) {
+            lxk::ladder_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes, u8b());
+        } else {
+            lxk::group_start_kernel<<<(h->lanes + 127) / 128, 128, 0, h->stream>>>(h->d_state, h->d_ns, d, h->lanes,
+                                                                                    h->batch / 2, u8b(), v8b());
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -292,19 +409,19 @@ int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args) {
     if (!h->initialised) return fail(h, LXMFV_ERR_STATE, "launch before init");
     if (args->iters == 0) return fail(h, LXMFV_ERR_ARG, "iters must be at least 1");
     if (int rc = set_device(h)) return rc;
-    lxk::WalkArgs wa;
-    memset(&wa, 0, sizeof wa);
-    wa.state = h->d_state;
-    wa.ns = h->d_ns;
-    wa.lanes = h->lanes;
-    wa.iters = args->iters;
-    for (int i = 0; i < 8; i++) wa.q.v[i] = args->q[i];
-    wa.q.v[7] &= 0x7fffffffu;
-    fill_addr_consts(wa.ac, args->ed, args->name_hash, args->want, args->mask);
+    // The step point is fixed: both walks' tables and start points are built
+    // from u(8B), so a launch must use it too (the reference passes it per
+    // launch, mod.rs:111).
+    fe q = u8b();
+    for (int i = 0; i < 8; i++)
+        if (args->q[i] != q.v[i]) return fail(h, LXMFV_ERR_ARG, "q must be u(8B), the walk's step point");
+    lxk::EmitArgs em;
+    memset(&em, 0, sizeof em);
+    fill_addr_consts(em.ac, args->ed, args->name_hash, args->want, args->mask);
     if (int rc = ensure_hits(h, std::max<uint32_t>(args->max_hits, 1))) return rc;
-    wa.hit_count = h->d_hit_count;
-    wa.hits = h->d_hits;
-    wa.max_hits = args->max_hits;
+    em.hit_count = h->d_hit_count;
+    em.hits = h->d_hits;
+    em.max_hits = args->max_hits;
     h->launch_max_hits = std::max(h->launch_max_hits, args->max_hits);
     if (args->dump_threads > 0) {
         const uint32_t dl = std::min(args->dump_threads, h->lanes);
@@ -313,16 +430,15 @@ int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args) {
             return fail(h, LXMFV_ERR_ARG, "dump_keys %u exceeds the %llu keys a lane walks in this launch", dk,
                         (unsigned long long)args->iters * h->batch);
         if (int rc = ensure_dump(h, (size_t)dl * dk)) return rc;
-        wa.dump_lanes = dl;
-        wa.dump_keys = dk;
-        wa.dump_u = h->d_dump_u;
-        wa.dump_addr = h->d_dump_addr;
+        em.dump_lanes = dl;
+        em.dump_keys = dk;
+        em.dump_u = h->d_dump_u;
+        em.dump_addr = h->d_dump_addr;
         h->dump_lanes = dl;
         h->dump_keys = dk;
     }
-    walk_fn fn = pick_walk(h->batch, h->block);
     CU(h, cudaEventRecord(h->ev0, h->stream));
-    fn<<<(h->lanes + h->block - 1) / h->block, h->block, 0, h->stream>>>(wa);
+    launch_walk(h, em, args->iters, q);
     CU(h, cudaGetLastError());
     CU(h, cudaEventRecord(h->ev1, h->stream));
     h->timed = true;

@@ -26,6 +26,8 @@ ERR_NOMEM = -3
 ERR_STATE = -4
 ERR_RECHECK = -5
 ERR_OVERFLOW = -6
+WALK_GROUP = 0
+WALK_XADD = 1
 
 # u(8B), the step point of the walk (mod.rs:111): 32 LE bytes.
 U8B = bytes.fromhex("6899c948ed6f71f11ea974adcaed787aa15cb6c84d883bd82d5cd6aad7a65f27")
@@ -41,7 +43,7 @@ class LxmfvError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("lanes", C.c_uint32), ("batch", C.c_uint32), ("block", C.c_uint32),
-                ("stream", C.c_void_p)]
+                ("walk", C.c_uint32), ("stream", C.c_void_p)]
 
 
 class LaunchArgs(C.Structure):
@@ -65,6 +67,7 @@ SIGNATURES = {
     "lxmfv_describe": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "lxmfv_threads": ([C.c_void_p], C.c_uint32),
     "lxmfv_batch": ([C.c_void_p], C.c_uint64),
+    "lxmfv_walk": ([C.c_void_p], C.c_uint32),
     "lxmfv_init": ([C.c_void_p, _u32p, C.c_size_t], C.c_int),
     "lxmfv_init_from_scalars": ([C.c_void_p, _u8p, C.c_size_t], C.c_int),
     "lxmfv_first_public_keys": ([C.c_void_p, _u8p, C.c_size_t, _u32p], C.c_int),
@@ -244,9 +247,10 @@ def make_launch_args(iters: int, ed_pub: bytes, prefix: tuple[bytes, int], aspec
 class Backend:
     """One open device: walker state for `threads()` lanes."""
 
-    def __init__(self, device: int = 0, lanes: int = 0, batch: int = 0, block: int = 0, stream: int | None = None):
+    def __init__(self, device: int = 0, lanes: int = 0, batch: int = 0, block: int = 0, stream: int | None = None,
+                 walk: int = 0):
         L = lib()
-        o = Options(device, lanes, batch, block, stream)
+        o = Options(device, lanes, batch, block, walk, stream)
         h = C.c_void_p()
         rc = L.lxmfv_open(C.byref(o), C.byref(h))
         self._h = h
@@ -287,6 +291,9 @@ class Backend:
 
     def batch(self) -> int:
         return lib().lxmfv_batch(self._h)
+
+    def walk(self) -> int:
+        return lib().lxmfv_walk(self._h)
 
     def init(self, u_prev_cur: np.ndarray) -> None:
         """Backend::init: 16 LE words per lane, u(k-8) then u(k)."""

@@ -28,9 +28,10 @@ def lx():
     return lxmfv
 
 
-@pytest.fixture(scope="session")
-def backend(lx):
-    """One open device for the GPU tests (a small walker count)."""
-    b = lx.Backend(device=0, lanes=4096, batch=64)
+@pytest.fixture(scope="session", params=["group", "xadd"])
+def backend(lx, request):
+    """One open device per walk for the GPU tests (a small walker count)."""
+    walk = lx.WALK_GROUP if request.param == "group" else lx.WALK_XADD
+    b = lx.Backend(device=0, lanes=4096, batch=64, walk=walk)
     yield b
     b.close()

@@ -27,7 +27,7 @@ def _hashes_of(dump_addr: np.ndarray, lanes: int, keys: int) -> np.ndarray:
 def test_describe(backend):
     d = backend.describe()
     assert "compute 10.0" in d and "SMs" in d
-    assert backend.threads() == 4096 and backend.batch() == 64
+    assert backend.threads() == 4096 and backend.batch() == 64 and backend.walk() in (0, 1)
 
 
 def test_field_small_golden(backend):
@@ -231,9 +231,11 @@ def test_other_aspects(backend, lx, oracle, aspect):
     assert set(hits) == expected
 
 
-@pytest.mark.parametrize("batch,block", [(16, 256), (32, 128), (128, 256)])
-def test_other_batch_sizes(lx, oracle, batch, block):
-    with lx.Backend(device=0, lanes=512, batch=batch, block=block) as b:
+@pytest.mark.parametrize("walk,batch,block", [(1, 16, 256), (1, 32, 128), (1, 128, 256),
+                                              (0, 32, 256), (0, 128, 128), (0, 256, 256)])
+def test_other_batch_sizes(lx, oracle, walk, batch, block):
+    with lx.Backend(device=0, lanes=512, batch=batch, block=block, walk=walk) as b:
+        assert b.walk() == walk and b.batch() == batch
         setup = lx.seeded_setup(808 + batch, 512)
         b.init_from_scalars(setup.scalars)
         args = lx.make_launch_args(2, setup.ed_pub, lx.prefix_parse("b0"), max_hits=1 << 14, dump_threads=3,
@@ -248,6 +250,31 @@ def test_other_batch_sizes(lx, oracle, batch, block):
                                         oracle.prefix_parse("b0"), 2 * batch)
             expected.update((t, int(x)) for x in h)
         assert set(hits) == expected
+
+
+def test_walks_agree_with_each_other(lx):
+    """The grouped and x-only walks give identical hits and dumps for the same lanes."""
+    out = []
+    for walk in (lx.WALK_GROUP, lx.WALK_XADD):
+        with lx.Backend(device=0, lanes=2048, batch=64, walk=walk) as b:
+            setup = lx.seeded_setup(999, 2048)
+            b.init_from_scalars(setup.scalars)
+            args = lx.make_launch_args(3, setup.ed_pub, lx.prefix_parse("0"), max_hits=1 << 16, dump_threads=2,
+                                       dump_keys=192)
+            hits, dump, dump_addr, n = b.launch(args, want_dump=True, want_dump_addr=True)
+            out.append((sorted(hits), dump, dump_addr, n))
+    assert out[0][0] == out[1][0] and out[0][3] == out[1][3] > 20000
+    assert (out[0][1] == out[1][1]).all() and (out[0][2] == out[1][2]).all()
+
+
+def test_bad_step_point_rejected(backend, lx):
+    setup = lx.seeded_setup(1, backend.threads())
+    backend.init_from_scalars(setup.scalars)
+    args = lx.make_launch_args(1, setup.ed_pub, lx.prefix_parse("b0"))
+    args.q[0] ^= 1
+    with pytest.raises(lx.LxmfvError) as e:
+        backend.launch(args)
+    assert e.value.code == lx.ERR_ARG
 
 
 def test_self_test_shape(lx):
