@@ -1,12 +1,13 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 key-walk search: keys/s on the plain GPU search.
 
-Workload (the plain GPU search): one 8-hex-digit prefix drawn from the seed,
+Workload (the plain GPU search): one 8-hex-digit prefix (numpy-seeded),
 aspect lxmf.delivery, every lane starting from its own seeded clamped X25519
-scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, B = 64 keys
-per inversion, 2^36 keys walked in total over the timed steps (a step is one
-launch that walks every lane `iters` batches further).  Synthetic, seeded
-inputs; no dataset is involved.
+scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, 2^36 keys
+walked in total over the timed steps (a step is one launch that walks every
+lane `iters` groups further).  Keys per inversion: the tuned 256 for the
+headline, and a second measurement at 64 (the reference kernel's BATCH) on a
+quarter of the keys.  Synthetic, seeded inputs; no dataset is involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -14,7 +15,8 @@ Prints one JSON line on rank 0.  `value` is device-timed (CUDA events on the
 launching stream, max over ranks), `e2e` goes through the C ABI's
 synchronous lxmfv_launch with host buffers, `cpu_baseline` is the restated
 CPU search on this host's cores, `roofline` relates the walk kernel's
-multiply work to the measured IMAD rate of this GPU.
+multiply work to the measured IMAD rate of this GPU, and
+`reference_cuda_kernel` times the reference's own CUDA kernel on this GPU.
 With --impl reference, the reference's own kernel body (src/gpu/common.h,
 built for the host) is timed on the host cores instead.
 """
@@ -33,15 +35,26 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "lxmf-vanity_b200"))
 
 TOTAL_KEYS = 1 << 36
-BATCH = 64
+BATCH = 256
 SEED = 3
-METRIC = "keys/s, plain GPU search (8-hex prefix, 2^36 keys, B=64), bit-exact"
+METRIC = "keys/s, plain GPU search (one 8-hex prefix, seeded walkers, 2^36 keys), bit-exact"
 
 
-def wide_products_per_key(b: int) -> float:
+def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
+    """(multiplies, squarings) per key, counted from the kernels' code.
+    x-only walk, B keys per inversion: 8B + 11 M and 2B + 254 S per batch.
+    Grouped walk, G = 2m keys per group: (5m + 13) M and (2m + 255) S per group."""
+    if walk == "xadd":
+        return 8 + 11 / b, 2 + 254 / b
+    m = b // 2
+    return (5 * m + 13) / b, (2 * m + 255) / b
+
+
+def wide_products_per_key(walk: str, b: int) -> float:
     """32x32->64 products per key with 8 x 32-bit limbs: a field multiply is
-    64 + 8 (fold by 38), a square 36 + 8; per key (8 + 11/B) M + (2 + 254/B) S."""
-    return (8 + 11 / b) * 72 + (2 + 254 / b) * 44
+    64 + 8 (the fold by 38), a square 36 + 8."""
+    mul, sqr = field_ops_per_key(walk, b)
+    return mul * 72 + sqr * 44
 
 
 def parse() -> argparse.Namespace:
@@ -51,12 +64,14 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--lanes", type=int, default=0, help="walker lanes per GPU (0: two full waves)")
-    p.add_argument("--batch", type=int, default=BATCH)
+    p.add_argument("--batch", type=int, default=BATCH, help="keys per inversion (grouped walk: 32..256)")
+    p.add_argument("--walk", choices=["group", "xadd"], default="group")
     p.add_argument("--block", type=int, default=0)
     p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
+    p.add_argument("--no-b64", action="store_true", help="skip the second measurement at B = 64")
     return p.parse_args()
 
 
@@ -228,29 +243,64 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = local
     torch.cuda.set_device(dev)
+    prefix = _prefix()
+    head = measure(torch, dist, lx, a, dev, rank, world, prefix, a.walk, a.batch, a.total_keys, a.steps, a.warmup,
+                   e2e=not a.no_e2e)
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": "keys/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded ChaCha20 starts, numpy-seeded prefix)",
+        "config": head["config"],
+        "gpu_launches": a.steps,
+        "e2e": head["e2e"],
+        "roofline": head["roofline"],
+        "clocks": head["clocks"],
+        "hits": head["hits"],
+        "start_points_s": head["start_points_s"],
+    }
+    if not a.no_b64 and a.batch != 64:
+        # The same workload at B = 64 keys per inversion, the reference kernel's
+        # batch (2^34 keys: a quarter of the headline's, to bound the run time).
+        b64 = measure(torch, dist, lx, a, dev, rank, world, prefix, a.walk, 64, a.total_keys / 4, a.steps,
+                      a.warmup, e2e=False)
+        line["at_batch_64"] = {"value": b64["value"], "unit": "keys/s", "ms_per_step": b64["ms_per_step"],
+                               "config": b64["config"], "clocks": b64["clocks"], "hits": b64["hits"]}
+    if rank == 0 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port(prefix)
+    if rank == 0 and not a.no_ref_cuda:
+        with lx.Backend(device=dev, lanes=1024) as b:
+            line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if head["hits"]["rechecked_bad"]:
+        sys.exit(f"{head['hits']['rechecked_bad']} GPU hits failed their CPU recheck")
+
+
+def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_keys, steps, warmup, e2e=True) -> dict:
+    """Times `steps` launches (after `warmup`) of the walk over `total_keys`
+    keys in all, device-timed with CUDA events on the launching stream."""
+    walk_id = lx.WALK_GROUP if walk == "group" else lx.WALK_XADD
     # A stream of our own (never the legacy default stream, whose handle is 0):
     # the library launches on it and the timing events are recorded on it.
     stream = torch.cuda.Stream(device=dev)
-    b = lx.Backend(device=dev, lanes=0, batch=a.batch, block=a.block, stream=stream.cuda_stream)
-    wave = b.threads()
-    b.close()
+    with lx.Backend(device=dev, lanes=0, batch=batch, block=a.block, walk=walk_id) as b0:
+        wave = b0.threads()
     lanes = a.lanes or wave * max(1, -(-131072 // wave))
-    b = lx.Backend(device=dev, lanes=lanes, batch=a.batch, block=a.block, stream=stream.cuda_stream)
-
-    prefix = _prefix()
+    b = lx.Backend(device=dev, lanes=lanes, batch=batch, block=a.block, walk=walk_id, stream=stream.cuda_stream)
     setup = lx.seeded_setup(SEED + 1000 * rank, lanes)
     t0 = time.perf_counter()
     b.init_from_scalars(setup.scalars)
     ladder_s = time.perf_counter() - t0
-    per_iter = lanes * a.batch
-    iters = max(1, round(a.total_keys / (a.steps * per_iter)))
+    per_iter = lanes * batch
+    iters = max(1, round(total_keys / (steps * per_iter)))
     keys_per_step = per_iter * iters
     args = lx.make_launch_args(iters, setup.ed_pub, lx.prefix_parse(prefix), max_hits=4096)
 
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         b.launch_async(args)
     b.collect()
-    kernel_ms_warm = b.last_kernel_ms()
 
     if world > 1:
         dist.barrier()
@@ -258,19 +308,17 @@ def main() -> None:
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev) as clk:
         ev0.record(stream)
-        for _ in range(a.steps):
+        for _ in range(steps):
             b.launch_async(args)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     ms = ev0.elapsed_time(ev1)
-    kernel_ms_last = b.last_kernel_ms()
     hits, n_hits = b.collect()
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    total_keys = keys_per_step * a.steps * world
-    value = total_keys / (ms * 1e-3)
+    value = keys_per_step * steps * world / (ms * 1e-3)
 
     # Every hit is rechecked from scratch on the CPU (OpenSSL), as the reference does.
     pfx = lx.prefix_parse(prefix)
@@ -278,9 +326,9 @@ def main() -> None:
 
     # End to end through the C ABI: synchronous lxmfv_launch per step, launch
     # arguments from the host, hit count and hits read back every step.
-    e2e = None
-    if not a.no_e2e:
-        e2e_steps = max(1, a.steps // 2)
+    e2e_line = None
+    if e2e:
+        e2e_steps = max(1, steps // 2)
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
@@ -294,46 +342,29 @@ def main() -> None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
         import ctypes
-        e2e = {"value": keys_per_step * e2e_steps * world / dt, "unit": "keys/s",
-               "h2d_bytes_per_step": ctypes.sizeof(lx.LaunchArgs), "d2h_bytes_per_step": d2h // e2e_steps,
-               "steps": e2e_steps, "api": "lxmfv_launch (C ABI, synchronous, host buffers)"}
+        e2e_line = {"value": keys_per_step * e2e_steps * world / dt, "unit": "keys/s",
+                    "h2d_bytes_per_step": ctypes.sizeof(lx.LaunchArgs), "d2h_bytes_per_step": d2h // e2e_steps,
+                    "steps": e2e_steps, "api": "lxmfv_launch (C ABI, synchronous, host buffers)"}
 
     imad_peak = b.peak_probe(0, 300.0)
     alu_peak = b.peak_probe(2, 300.0)
-    kernel_s = ms * 1e-3 / a.steps
-    prods = wide_products_per_key(a.batch)
-    achieved = 2 * prods * keys_per_step / kernel_s  # lo + hi IMAD per 32x32->64 product
-    line = {
-        "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32", "data": "synthetic (seeded ChaCha20 starts)",
-        "config": {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, B=64, 2^36 keys per run)",
-                   "prefix": prefix, "lanes_per_gpu": lanes, "batch": a.batch, "iters_per_step": iters,
-                   "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
-                   "l2": "working set (lane state + per-lane batch buffers) exceeds L2; no flush needed"},
-        "gpu_launches": a.steps,
-        "e2e": e2e,
-        "roofline": {"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
-                     "frac": achieved / imad_peak, "traffic": None,
-                     "note": f"algorithmic {2 * prods:.0f} IMAD (lo+hi of {prods:.0f} 32x32->64 products) per key; "
-                             f"peak = measured mad.lo.u32 rate of this GPU (probe)",
-                     "alu_peak_T": alu_peak / 1e12},
-        "clocks": clk.summary(),
-        "hits": {"found": int(n_hits), "rechecked_bad": len(bad)},
-        "start_points_s": ladder_s,
-        "kernel_ms": {"warm_last": kernel_ms_warm, "timed_last": kernel_ms_last},
-    }
-    if rank == 0 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_port(prefix)
-    if rank == 0 and not a.no_ref_cuda:
-        line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)
     b.close()
-    if world > 1:
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if bad:
-        sys.exit(f"{len(bad)} GPU hits failed their CPU recheck")
+    kernel_s = ms * 1e-3 / steps
+    mul, sqr = field_ops_per_key(walk, batch)
+    prods = wide_products_per_key(walk, batch)
+    achieved = 2 * prods * keys_per_step / kernel_s  # lo + hi IMAD per 32x32->64 product
+    roofline = {"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
+                "frac": achieved / imad_peak, "traffic": None,
+                "note": f"algorithmic {mul:.2f} M + {sqr:.2f} S = {prods:.0f} 32x32->64 products "
+                        f"(lo + hi IMAD each) per key; peak = measured mad.lo.u32 rate of this GPU (probe)",
+                "alu_peak": alu_peak / 1e12}
+    config = {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, seeded walkers, 2^36 keys per run)",
+              "walk": walk, "prefix": prefix, "lanes_per_gpu": lanes, "batch": batch, "iters_per_step": iters,
+              "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
+              "l2": "working set (lane state + per-lane batch buffers) exceeds L2; no flush needed"}
+    return {"value": value, "ms_per_step": ms / steps, "e2e": e2e_line, "roofline": roofline,
+            "clocks": clk.summary(), "hits": {"found": int(n_hits), "rechecked_bad": len(bad)},
+            "start_points_s": ladder_s, "config": config}
 
 
 def _prefix() -> str:

@@ -49,6 +49,11 @@ typedef struct lxmfv_handle lxmfv_handle;
 #define LXMFV_WALK_XADD 1
 #define LXMFV_MAX_HALF_GROUP 128
 
+/* Option flags.  PHASE_SYNC (grouped walk, blocks of 256 or 512): a block
+ * barrier after every group keeps a block's warps in the same phase of the
+ * walk, so they share one phase's code in the instruction cache. */
+#define LXMFV_FLAG_PHASE_SYNC 1u
+
 /* Opening options; zero fields take defaults.
  * Replaces the constants of src/gpu/cuda.rs:13-16 (BATCH, BLOCK,
  * THREADS_PER_SM) and CudaContext::new(0) (cuda.rs:33-64). */
@@ -56,8 +61,9 @@ typedef struct {
     int32_t device;       /* CUDA device ordinal */
     uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
     uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32, 64, 128, 256; 0: 64 */
-    uint32_t block;       /* threads per block: 128 or 256; 0: 256 */
+    uint32_t block;       /* threads per block: 128, 256 (512: grouped walk only); 0: 256 */
     uint32_t walk;        /* LXMFV_WALK_GROUP (0, default) or LXMFV_WALK_XADD */
+    uint32_t flags;       /* LXMFV_FLAG_* */
     void* stream;         /* cudaStream_t to launch on; NULL: a stream of the handle's own */
 } lxmfv_options;
 

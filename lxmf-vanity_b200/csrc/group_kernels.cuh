@@ -133,10 +133,16 @@ __global__ void __launch_bounds__(128) group_init_kernel(uint32_t* state, uint64
     ns[lane] = 0;
 }
 
-template <int M, int BLOCK, int MINB>
+// SYNC: a block barrier after each group keeps the block's warps in the same
+// phase of the walk, so that they share the instruction cache's working set
+// (one phase's code instead of all of it).  Threads past the last lane then
+// walk a copy of the last lane and neither emit nor store.
+template <int M, int BLOCK, int MINB, bool SYNC>
 __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ GroupArgs<M> a) {
-    const uint32_t lane = blockIdx.x * BLOCK + threadIdx.x;
-    if (lane >= a.lanes) return;
+    const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
+    if (!SYNC && tid >= a.lanes) return;
+    const bool active = tid < a.lanes;
+    const uint32_t lane = active ? tid : a.lanes - 1;
     fe uc = load_fe(a.state, 0, lane, a.lanes);
     fe vc = load_fe(a.state, 1, lane, a.lanes);
     const uint64_t key0 = a.ns[lane];
@@ -183,7 +189,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_co
                 // side 1: key c - i (i = 0: the centre).
                 if (side == 1 || (i > 0 && i < M)) {
                     const fe u = fe_canon(side ? um : up);
-                    emit_key(a.em, lane, side ? c - (uint64_t)i : c + (uint64_t)i, key0, u);
+                    if (active) emit_key(a.em, lane, side ? c - (uint64_t)i : c + (uint64_t)i, key0, u);
                 }
             }
             if (i == 0) {
@@ -192,11 +198,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_co
             }
         }
         n += 2 * M;
+        if (SYNC) __syncthreads();
     }
 
-    store_fe(a.state, 0, lane, a.lanes, uc);
-    store_fe(a.state, 1, lane, a.lanes, vc);
-    a.ns[lane] = n;
+    if (active) {
+        store_fe(a.state, 0, lane, a.lanes, uc);
+        store_fe(a.state, 1, lane, a.lanes, vc);
+        a.ns[lane] = n;
+    }
 }
 
 }  // namespace lxk

@@ -31,6 +31,7 @@ struct lxmfv_handle {
     uint32_t lanes = 0;
     uint32_t batch = 64;  // keys per inversion: B (x-only walk) or G = 2M (grouped walk)
     uint32_t block = 256;
+    bool sync = false;    // grouped walk: block barrier after each group
     uint32_t* d_state = nullptr;
     uint64_t* d_ns = nullptr;
     uint32_t* d_hit_count = nullptr;
@@ -68,34 +69,60 @@ int fail(lxmfv_handle* h, int code, const char* fmt, ...) {
                         __FILE__, __LINE__);                                                 \
     } while (0)
 
-constexpr int minb(int block) { return block == 256 ? 2 : 4; }
+constexpr int minb(int block) { return block == 512 ? 1 : block == 256 ? 2 : 4; }
 
-// The walk kernel of a configuration, for the occupancy query.
-const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block) {
-#define LXMFV_X(B)                                                                                   \
-    if (batch == B)                                                                                  \
-        return block == 128 ? (const void*)lxk::walk_kernel<B, 128, minb(128)>                       \
-                            : (const void*)lxk::walk_kernel<B, 256, minb(256)>;
-#define LXMFV_G(G)                                                                                   \
-    if (batch == G)                                                                                  \
-        return block == 128 ? (const void*)lxk::group_walk_kernel<G / 2, 128, minb(128)>             \
-                            : (const void*)lxk::group_walk_kernel<G / 2, 256, minb(256)>;
-    if (block != 128 && block != 256) return nullptr;
+// The kernels for a configuration: block 128 runs without the phase barrier;
+// 256 and 512 with or without it.
+template <int M>
+const void* group_kernel_ptr(uint32_t block, bool sync) {
+    if (block == 128) return (const void*)lxk::group_walk_kernel<M, 128, minb(128), false>;
+    if (block == 256)
+        return sync ? (const void*)lxk::group_walk_kernel<M, 256, minb(256), true>
+                    : (const void*)lxk::group_walk_kernel<M, 256, minb(256), false>;
+    if (block == 512)
+        return sync ? (const void*)lxk::group_walk_kernel<M, 512, minb(512), true>
+                    : (const void*)lxk::group_walk_kernel<M, 512, minb(512), false>;
+    return nullptr;
+}
+
+template <int B>
+const void* xadd_kernel_ptr(uint32_t block, bool sync) {
+    if (block == 128) return (const void*)lxk::walk_kernel<B, 128, minb(128), false>;
+    if (block == 256)
+        return sync ? (const void*)lxk::walk_kernel<B, 256, minb(256), true>
+                    : (const void*)lxk::walk_kernel<B, 256, minb(256), false>;
+    if (block == 512)
+        return sync ? (const void*)lxk::walk_kernel<B, 512, minb(512), true>
+                    : (const void*)lxk::walk_kernel<B, 512, minb(512), false>;
+    return nullptr;
+}
+
+// The walk kernel of a configuration (null when unsupported).
+const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync) {
     if (walk == LXMFV_WALK_XADD) {
-        LXMFV_X(16) LXMFV_X(32) LXMFV_X(64) LXMFV_X(128)
+        switch (batch) {
+            case 16: return xadd_kernel_ptr<16>(block, sync);
+            case 32: return xadd_kernel_ptr<32>(block, sync);
+            case 64: return xadd_kernel_ptr<64>(block, sync);
+            case 128: return xadd_kernel_ptr<128>(block, sync);
+        }
     } else if (walk == LXMFV_WALK_GROUP) {
-        LXMFV_G(32) LXMFV_G(64) LXMFV_G(128) LXMFV_G(256)
+        switch (batch) {
+            case 32: return group_kernel_ptr<16>(block, sync);
+            case 64: return group_kernel_ptr<32>(block, sync);
+            case 128: return group_kernel_ptr<64>(block, sync);
+            case 256: return group_kernel_ptr<128>(block, sync);
+        }
     }
-#undef LXMFV_X
-#undef LXMFV_G
     return nullptr;
 }
 
 template <int B>
 void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
-    if (h->block == 128) lxk::walk_kernel<B, 128, minb(128)><<<grid, 128, 0, h->stream>>>(wa);
-    else lxk::walk_kernel<B, 256, minb(256)><<<grid, 256, 0, h->stream>>>(wa);
+    typedef void (*fn_t)(lxk::WalkArgs);
+    const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync);
+    fn<<<grid, h->block, 0, h->stream>>>(wa);
 }
 
 template <int M>
@@ -111,8 +138,9 @@ void launch_group(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
         ga.t.v[i] = h->tv[i];
     }
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
-    if (h->block == 128) lxk::group_walk_kernel<M, 128, minb(128)><<<grid, 128, 0, h->stream>>>(ga);
-    else lxk::group_walk_kernel<M, 256, minb(256)><<<grid, 256, 0, h->stream>>>(ga);
+    typedef void (*fn_t)(lxk::GroupArgs<M>);
+    const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync);
+    fn<<<grid, h->block, 0, h->stream>>>(ga);
 }
 
 void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const fe& q) {
@@ -143,6 +171,7 @@ void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const
 
 void fill_addr_consts(lxsha::AddrConsts& ac, const uint32_t ed[8], const uint32_t nh[3], const uint32_t want[4],
                       const uint32_t mask[4]) {
+    ac.one = 1;
     for (int i = 0; i < 8; i++) ac.ed[i] = ed ? ed[i] : 0;
     for (int i = 0; i < 3; i++) ac.nh[i] = nh[i];
     for (int i = 0; i < 4; i++) {
@@ -260,13 +289,16 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     h->device = o.device;
     h->walk = o.walk;
     h->batch = o.batch ? o.batch : 64;
-    h->block = o.block ? o.block : 256;
+    // Default launch shape (block 0): 512 threads with the phase barrier, the
+    // fastest measured on B200 for both walks; otherwise the flags decide.
+    h->block = o.block ? o.block : 512;
+    h->sync = o.block ? (o.flags & LXMFV_FLAG_PHASE_SYNC) != 0 : true;
     if (h->walk != LXMFV_WALK_GROUP && h->walk != LXMFV_WALK_XADD)
         return fail(h, LXMFV_ERR_ARG, "walk %u: 0 grouped, 1 x-only", h->walk);
-    if (!walk_kernel_ptr(h->walk, h->batch, h->block))
+    if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync))
         return fail(h, LXMFV_ERR_ARG,
-                    "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: 32, 64, "
-                    "128, 256; block 128 or 256)",
+                    "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
+                    "batch 32, 64, 128, 256; block 128, 256 or 512)",
                     h->batch, h->block);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -293,7 +325,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     CU(h, cudaEventCreate(&h->ev0));
     CU(h, cudaEventCreate(&h->ev1));
     int per_sm = 0;
-    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block),
+    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block, h->sync),
                                                         (int)h->block, 0));
     if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
     h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;

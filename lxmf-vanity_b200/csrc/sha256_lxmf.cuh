@@ -50,20 +50,38 @@ __device__ __forceinline__ uint32_t ssig1(uint32_t w) { return rotr(w, 17) ^ rot
 __device__ __forceinline__ uint32_t ch(uint32_t e, uint32_t f, uint32_t g) { return (e & f) ^ (~e & g); }
 __device__ __forceinline__ uint32_t maj(uint32_t a, uint32_t b, uint32_t c) { return (a & b) | (c & (a | b)); }
 
-// One round: the new e lands in d and the new a in h (the caller rotates names).
-#define LXSHA_R(a, b, c, d, e, f, g, h, kw)                          \
-    {                                                                \
-        const uint32_t t1_ = h + bsig1(e) + ch(e, f, g) + (kw);      \
-        d += t1_;                                                    \
-        h = t1_ + bsig0(a) + maj(a, b, c);                           \
+// Additions on the multiply-add pipe.  The chain is bound by the integer ALU
+// pipe (rotates, LOP3, IADD3) while the IMAD pipe idles, so two-input sums
+// off the round's critical path are issued as x * one + y, with `one` a
+// runtime 1 (a kernel parameter) that the compiler cannot fold back into an
+// IADD3.
+__device__ __forceinline__ uint32_t madd(uint32_t x, uint32_t y, uint32_t one) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(one), "r"(y));
+    return r;
+}
+
+// One round: the new e lands in d and the new a in h (the caller rotates
+// names).  h + K + W and Sigma0 + Maj go to the IMAD pipe; the sum that
+// joins Sigma1 and Ch stays one IADD3 on the critical path.
+#define LXSHA_R(a, b, c, d, e, f, g, h, kw)                                \
+    {                                                                      \
+        const uint32_t hk_ = madd(h, (kw), one);                           \
+        const uint32_t t1_ = hk_ + bsig1(e) + ch(e, f, g);                 \
+        const uint32_t s0m_ = madd(bsig0(a), maj(a, b, c), one);           \
+        d = madd(d, t1_, one);                                             \
+        h = madd(t1_, s0m_, one);                                          \
     }
 
-#define LXSHA_SCHED(w, r) (w[(r)] += ssig0(w[((r) + 1) & 15]) + w[((r) + 9) & 15] + ssig1(w[((r) + 14) & 15]))
+#define LXSHA_SCHED(w, r)                                                                           \
+    (w[(r)] = madd(madd(madd(w[(r)], w[((r) + 9) & 15], one), ssig0(w[((r) + 1) & 15]), one),     \
+                   ssig1(w[((r) + 14) & 15]), one))
 
 // 16 rounds with message words (SCHED: extend the schedule in place first).
 template <bool SCHED>
 __device__ __forceinline__ void rounds16(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t& e,
-                                         uint32_t& f, uint32_t& g, uint32_t& h, uint32_t w[16], const uint32_t* k) {
+                                         uint32_t& f, uint32_t& g, uint32_t& h, uint32_t w[16], const uint32_t* k,
+                                         uint32_t one) {
 #pragma unroll
     for (int half = 0; half < 2; half++) {
         const int r = 8 * half;
@@ -71,20 +89,21 @@ __device__ __forceinline__ void rounds16(uint32_t& a, uint32_t& b, uint32_t& c, 
 #pragma unroll
             for (int i = 0; i < 8; i++) LXSHA_SCHED(w, r + i);
         }
-        LXSHA_R(a, b, c, d, e, f, g, h, k[r + 0] + w[r + 0]);
-        LXSHA_R(h, a, b, c, d, e, f, g, k[r + 1] + w[r + 1]);
-        LXSHA_R(g, h, a, b, c, d, e, f, k[r + 2] + w[r + 2]);
-        LXSHA_R(f, g, h, a, b, c, d, e, k[r + 3] + w[r + 3]);
-        LXSHA_R(e, f, g, h, a, b, c, d, k[r + 4] + w[r + 4]);
-        LXSHA_R(d, e, f, g, h, a, b, c, k[r + 5] + w[r + 5]);
-        LXSHA_R(c, d, e, f, g, h, a, b, k[r + 6] + w[r + 6]);
-        LXSHA_R(b, c, d, e, f, g, h, a, k[r + 7] + w[r + 7]);
+        LXSHA_R(a, b, c, d, e, f, g, h, madd(w[r + 0], k[r + 0], one));
+        LXSHA_R(h, a, b, c, d, e, f, g, madd(w[r + 1], k[r + 1], one));
+        LXSHA_R(g, h, a, b, c, d, e, f, madd(w[r + 2], k[r + 2], one));
+        LXSHA_R(f, g, h, a, b, c, d, e, madd(w[r + 3], k[r + 3], one));
+        LXSHA_R(e, f, g, h, a, b, c, d, madd(w[r + 4], k[r + 4], one));
+        LXSHA_R(d, e, f, g, h, a, b, c, madd(w[r + 5], k[r + 5], one));
+        LXSHA_R(c, d, e, f, g, h, a, b, madd(w[r + 6], k[r + 6], one));
+        LXSHA_R(b, c, d, e, f, g, h, a, madd(w[r + 7], k[r + 7], one));
     }
 }
 
 // 16 rounds whose K + W words are given (a constant message).
 __device__ __forceinline__ void rounds16_kw(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t& e,
-                                            uint32_t& f, uint32_t& g, uint32_t& h, const uint32_t* kw) {
+                                            uint32_t& f, uint32_t& g, uint32_t& h, const uint32_t* kw,
+                                            uint32_t one) {
 #pragma unroll
     for (int half = 0; half < 2; half++) {
         const int r = 8 * half;
@@ -101,19 +120,19 @@ __device__ __forceinline__ void rounds16_kw(uint32_t& a, uint32_t& b, uint32_t& 
 
 // 64 rounds over message w (overwritten by the schedule); s in, working
 // state out (the caller adds the chaining value).
-__device__ __forceinline__ void compress(uint32_t s[8], uint32_t w[16]) {
+__device__ __forceinline__ void compress(uint32_t s[8], uint32_t w[16], uint32_t one) {
     uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
-    rounds16<false>(a, b, c, d, e, f, g, h, w, K);
+    rounds16<false>(a, b, c, d, e, f, g, h, w, K, one);
 #pragma unroll 1
-    for (int j = 1; j < 4; j++) rounds16<true>(a, b, c, d, e, f, g, h, w, K + 16 * j);
+    for (int j = 1; j < 4; j++) rounds16<true>(a, b, c, d, e, f, g, h, w, K + 16 * j, one);
     s[0] = a; s[1] = b; s[2] = c; s[3] = d; s[4] = e; s[5] = f; s[6] = g; s[7] = h;
 }
 
 // 64 rounds of the constant padding block.
-__device__ __forceinline__ void compress_pad64(uint32_t s[8]) {
+__device__ __forceinline__ void compress_pad64(uint32_t s[8], uint32_t one) {
     uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
 #pragma unroll 1
-    for (int j = 0; j < 4; j++) rounds16_kw(a, b, c, d, e, f, g, h, kKW2 + 16 * j);
+    for (int j = 0; j < 4; j++) rounds16_kw(a, b, c, d, e, f, g, h, kKW2 + 16 * j, one);
     s[0] = a; s[1] = b; s[2] = c; s[3] = d; s[4] = e; s[5] = f; s[6] = g; s[7] = h;
 }
 
@@ -132,6 +151,7 @@ struct AddrConsts {
     uint32_t nh[3];     // name hash, big-endian words; nh[2] holds bytes 8, 9 in its top half
     uint32_t want[4];   // prefix compare: (dest[k] & mask[k]) == want[k]
     uint32_t mask[4];
+    uint32_t one;       // 1 (see madd)
 };
 
 __device__ __forceinline__ void iv(uint32_t s[8]) {
@@ -145,6 +165,7 @@ __device__ __forceinline__ void iv(uint32_t s[8]) {
 __device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi[8], const AddrConsts& c,
                                           uint32_t out[4]) {
     uint32_t w[16], s[8];
+    const uint32_t one = c.one;
     // Block 1: u (byte-swapped to big-endian words) || Ed25519 key.
 #pragma unroll
     for (int i = 0; i < 8; i++) w[i] = __byte_perm(u[i], 0, 0x0123);
@@ -153,7 +174,7 @@ __device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi
     iv(s);
 #pragma unroll 1
     for (int pass = 0;; pass++) {
-        compress(s, w);
+        compress(s, w, one);
         if (pass == 1) break;
         // Block 2: the padding block, chained from block 1.
         uint32_t h1[8], t[8];
@@ -161,7 +182,7 @@ __device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi
         h1[4] = s[4] + LXSHA_IV4; h1[5] = s[5] + LXSHA_IV5; h1[6] = s[6] + LXSHA_IV6; h1[7] = s[7] + LXSHA_IV7;
 #pragma unroll
         for (int i = 0; i < 8; i++) t[i] = h1[i];
-        compress_pad64(t);
+        compress_pad64(t, one);
         const uint32_t ih0 = t[0] + h1[0], ih1 = t[1] + h1[1], ih2 = t[2] + h1[2], ih3 = t[3] + h1[3];
         // Block 3: name_hash (10) || identity hash (16) || padding, 208 bits.
         w[0] = c.nh[0];

@@ -102,10 +102,15 @@ __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint6
     }
 }
 
-template <int B, int BLOCK, int MINB>
+// SYNC: a block barrier after each batch keeps the block's warps in the same
+// phase (see group_walk_kernel); threads past the last lane then walk a copy
+// of the last lane and neither emit nor store.
+template <int B, int BLOCK, int MINB, bool SYNC>
 __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant__ WalkArgs a) {
-    const uint32_t lane = blockIdx.x * BLOCK + threadIdx.x;
-    if (lane >= a.lanes) return;
+    const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
+    if (!SYNC && tid >= a.lanes) return;
+    const bool active = tid < a.lanes;
+    const uint32_t lane = active ? tid : a.lanes - 1;
     fe xp = load_fe(a.state, 0, lane, a.lanes);
     fe zp = load_fe(a.state, 1, lane, a.lanes);
     fe xc = load_fe(a.state, 2, lane, a.lanes);
@@ -136,16 +141,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant
         for (int i = B - 1; i >= 0; --i) {
             const fe u = fe_canon(fe_mul(ys[i], inv));
             inv = fe_mul(inv, zs[i]);
-            emit_key(a.em, lane, n + (uint64_t)i, key0, u);
+            if (active) emit_key(a.em, lane, n + (uint64_t)i, key0, u);
         }
         n += B;
+        if (SYNC) __syncthreads();
     }
 
-    store_fe(a.state, 0, lane, a.lanes, xp);
-    store_fe(a.state, 1, lane, a.lanes, zp);
-    store_fe(a.state, 2, lane, a.lanes, xc);
-    store_fe(a.state, 3, lane, a.lanes, zc);
-    a.ns[lane] = n;
+    if (active) {
+        store_fe(a.state, 0, lane, a.lanes, xp);
+        store_fe(a.state, 1, lane, a.lanes, zp);
+        store_fe(a.state, 2, lane, a.lanes, xc);
+        store_fe(a.state, 3, lane, a.lanes, zc);
+        a.ns[lane] = n;
+    }
 }
 
 // Backend::init (mod.rs:48): lane t from u(k-8), u(k) as 16 LE words, Z = 1.

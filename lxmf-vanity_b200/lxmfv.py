@@ -28,6 +28,7 @@ ERR_RECHECK = -5
 ERR_OVERFLOW = -6
 WALK_GROUP = 0
 WALK_XADD = 1
+FLAG_PHASE_SYNC = 1
 
 # u(8B), the step point of the walk (mod.rs:111): 32 LE bytes.
 U8B = bytes.fromhex("6899c948ed6f71f11ea974adcaed787aa15cb6c84d883bd82d5cd6aad7a65f27")
@@ -43,7 +44,7 @@ class LxmfvError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("lanes", C.c_uint32), ("batch", C.c_uint32), ("block", C.c_uint32),
-                ("walk", C.c_uint32), ("stream", C.c_void_p)]
+                ("walk", C.c_uint32), ("flags", C.c_uint32), ("stream", C.c_void_p)]
 
 
 class LaunchArgs(C.Structure):
@@ -248,9 +249,9 @@ class Backend:
     """One open device: walker state for `threads()` lanes."""
 
     def __init__(self, device: int = 0, lanes: int = 0, batch: int = 0, block: int = 0, stream: int | None = None,
-                 walk: int = 0):
+                 walk: int = 0, flags: int = 0):
         L = lib()
-        o = Options(device, lanes, batch, block, walk, stream)
+        o = Options(device, lanes, batch, block, walk, flags, stream)
         h = C.c_void_p()
         rc = L.lxmfv_open(C.byref(o), C.byref(h))
         self._h = h

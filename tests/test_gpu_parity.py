@@ -252,6 +252,32 @@ def test_other_batch_sizes(lx, oracle, walk, batch, block):
         assert set(hits) == expected
 
 
+@pytest.mark.parametrize("block", [256, 512])
+def test_phase_sync_with_a_partial_block(lx, oracle, block):
+    """The block-barrier variant with lanes that do not fill the last block:
+    the spare threads walk a copy of the last lane and must not emit or store."""
+    lanes = 1000
+    with lx.Backend(device=0, lanes=lanes, batch=64, block=block, flags=lx.FLAG_PHASE_SYNC) as b:
+        setup = lx.seeded_setup(4242, lanes)
+        b.init_from_scalars(setup.scalars)
+        for launch in range(2):
+            args = lx.make_launch_args(2, setup.ed_pub, lx.prefix_parse("a"), max_hits=1 << 14, dump_threads=lanes,
+                                       dump_keys=128)
+            hits, dump, _, n = b.launch(args, want_dump=True)
+            assert n == len(hits)
+            keys = _keys_of(dump, lanes, 128)
+            for t in (0, 1, 511, 998, 999):
+                walked = oracle.walk_keys(bytes(setup.scalars[t]), 256)
+                assert (keys[t] == walked[128 * launch:128 * (launch + 1)]).all(), (t, launch)
+            assert all(t < lanes for t, _ in hits)
+            expected = set()
+            for t in range(lanes):
+                h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, oracle.name_hash(),
+                                            oracle.prefix_parse("a"), 256)
+                expected.update((t, int(x)) for x in h if 128 * launch <= x < 128 * (launch + 1))
+            assert set(hits) == expected
+
+
 def test_walks_agree_with_each_other(lx):
     """The grouped and x-only walks give identical hits and dumps for the same lanes."""
     out = []
