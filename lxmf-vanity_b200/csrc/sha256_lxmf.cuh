@@ -62,12 +62,17 @@ __device__ __forceinline__ uint32_t madd(uint32_t x, uint32_t y, uint32_t one) {
 }
 
 // One round: the new e lands in d and the new a in h (the caller rotates
-// names).  h + K + W and Sigma0 + Maj go to the IMAD pipe; the sum that
-// joins Sigma1 and Ch stays one IADD3 on the critical path.
+// names).  Every sum is a two-input IMAD; the ALU pipe keeps only the
+// rotates and the LOP3s of Sigma0, Sigma1, Ch and Maj.
+#ifndef LXSHA_T1_ON_ALU
+#define LXSHA_T1(hk, s1, chv) madd(madd(hk, s1, one), chv, one)
+#else
+#define LXSHA_T1(hk, s1, chv) ((hk) + (s1) + (chv))
+#endif
 #define LXSHA_R(a, b, c, d, e, f, g, h, kw)                                \
     {                                                                      \
         const uint32_t hk_ = madd(h, (kw), one);                           \
-        const uint32_t t1_ = hk_ + bsig1(e) + ch(e, f, g);                 \
+        const uint32_t t1_ = LXSHA_T1(hk_, bsig1(e), ch(e, f, g));         \
         const uint32_t s0m_ = madd(bsig0(a), maj(a, b, c), one);           \
         d = madd(d, t1_, one);                                             \
         h = madd(t1_, s0m_, one);                                          \

@@ -17,7 +17,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "liblxmfv.so")
+# LXMFV_LIB names another build of the library (e.g. a variant under test).
+LIB_PATH = os.environ.get("LXMFV_LIB") or os.path.join(PKG, "liblxmfv.so")
 
 OK = 0
 ERR_ARG = -1
