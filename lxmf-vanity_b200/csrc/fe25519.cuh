@@ -204,8 +204,8 @@ __device__ __constant__ uint8_t kInvSq[11] = {2, 0, 1, 5, 10, 20, 10, 50, 100, 5
 __device__ __constant__ uint8_t kInvOp[11] = {0, 1, 2, 6, 6, 6, 4, 6, 6, 5, 3};
 __device__ __constant__ uint8_t kInvSave[11] = {2, 3, 0, 4, 0, 0, 5, 0, 0, 0, 0};
 
-// z^(p-2).  0 maps to 0.
-__device__ __noinline__ fe fe_invert(fe z) {
+// z^(p-2).  0 maps to 0.  (static: each translation unit has its own copy.)
+static __device__ __noinline__ fe fe_invert(fe z) {
     fe z2 = fe_sqr(z);
     fe z9 = z, z11 = z, z10 = z, z50 = z;
     fe t = z2;

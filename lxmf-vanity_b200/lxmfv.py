@@ -94,7 +94,19 @@ SIGNATURES = {
     "lxmfv_fe_op": ([C.c_void_p, C.c_int, _u32p, _u32p, _u32p, C.c_uint64, C.c_uint32], C.c_int),
     "lxmfv_address_chain": ([C.c_void_p, _u8p, _u8p, _u8p, C.c_uint64], C.c_int),
     "lxmfv_peak_probe": ([C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_double)], C.c_int),
+    "lxmfv_fe_batch_invert_static": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_char_p,
+                                      C.c_size_t], C.c_int),
 }
+STATIC_SCRATCH_ELEMS = 131072
+
+
+def fe_batch_invert_static(d_a: int, d_out: int, count: int, group: int = 64, stream: int | None = None) -> None:
+    """lxmfv_fe_batch_invert_static on device pointers (no device allocation;
+    asynchronous on `stream`).  Raises LxmfvError with the library's message."""
+    err = C.create_string_buffer(256)
+    rc = lib().lxmfv_fe_batch_invert_static(d_a, d_out, count, group, stream, err, 256)
+    if rc != OK:
+        raise LxmfvError(rc, err.value.decode())
 
 
 def lib():
