@@ -159,6 +159,78 @@ float lxmfv_last_kernel_ms(const lxmfv_handle* h);
 /* Releases the handle and its device memory (NULL is ignored). */
 void lxmfv_close(lxmfv_handle* h);
 
+/* ---- The search pool: many searches in one persistent kernel. ----
+ * No counterpart in the reference, which runs one search per process
+ * (GpuSearch, mod.rs:86-174) and starts more processes to search more
+ * (fleet.sh).  Searches with different prefixes, aspects and identities are
+ * admitted into a device-resident pool of walker lanes, walked together by a
+ * persistent kernel that takes 32-lane chunks from a device work queue, and
+ * retired as their hits come in.  Every step advances every active lane by
+ * the same number of keys, so a search's hits do not depend on the rest of
+ * the pool.  A step is a CUDA graph (reset, persistent kernel, hit read-back)
+ * captured once per step length. */
+typedef struct lxmfv_pool lxmfv_pool;
+
+typedef struct {
+    int32_t device;
+    uint32_t capacity_lanes; /* walker lanes in the pool; 0: memory_budget / bytes per lane, else 2^20 */
+    uint64_t memory_budget;  /* device bytes for lanes (108 per lane) when capacity_lanes is 0 */
+    uint32_t batch;          /* keys per group: 64, 128 or 256; 0: 256 */
+    uint32_t max_searches;   /* search slots; 0: 4096 */
+    uint32_t max_hits;       /* hits held between polls; 0: 65536 */
+    void* stream;            /* cudaStream_t; NULL: a stream of the pool's own */
+} lxmfv_pool_options;
+
+/* One search: the launch arguments' per-search fields (LaunchArgs,
+ * mod.rs:29-38) and its number of lanes (a multiple of 32). */
+typedef struct {
+    uint32_t ed[8];
+    uint32_t name_hash[3];
+    uint32_t want[4];
+    uint32_t mask[4];
+    uint32_t lanes;
+} lxmfv_search_desc;
+
+/* A hit: search id, lane within the search, walk index.  The identity is
+ * step_scalar(scalars[lane], n) || the search's Ed25519 seed. */
+typedef struct {
+    uint32_t search;
+    uint32_t lane;
+    uint64_t n;
+} lxmfv_pool_hit;
+
+typedef struct {
+    uint32_t capacity_lanes, free_lanes, active_searches, active_lanes, batch, sms;
+} lxmfv_pool_info_t;
+
+int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out);
+const char* lxmfv_pool_last_error(const lxmfv_pool* p);
+int lxmfv_pool_info(const lxmfv_pool* p, lxmfv_pool_info_t* info);
+
+/* Admits a search: `scalars` holds desc->lanes start scalars (32 LE bytes
+ * each, clamped).  LXMFV_ERR_OVERFLOW when the pool has too few free lanes or
+ * no free slot (admission against the memory budget). */
+int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* desc, const uint8_t* scalars, uint32_t* search_id);
+
+/* Frees a search's lanes; it takes no further part in steps. */
+int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id);
+
+/* Enqueues one step: every active lane walks `groups` groups (groups *
+ * batch keys).  Asynchronous. */
+int lxmfv_pool_step(lxmfv_pool* p, uint32_t groups);
+
+/* Waits for the enqueued steps and returns the hits found since the last
+ * poll (up to cap; *n_hits is their total, which may exceed cap). */
+int lxmfv_pool_poll(lxmfv_pool* p, lxmfv_pool_hit* hits, uint32_t cap, uint32_t* n_hits);
+
+/* The walk index every lane of a search has reached (keys walked per lane). */
+uint64_t lxmfv_pool_keys_per_lane(const lxmfv_pool* p, uint32_t search_id);
+
+/* Device time of the last step in milliseconds (CUDA events). */
+float lxmfv_pool_last_step_ms(const lxmfv_pool* p);
+
+void lxmfv_pool_close(lxmfv_pool* p);
+
 /* ---- Host helpers (CPU): the reference's address and scalar rules. ---- */
 
 /* Prefix::parse (main.rs:206-216): 1..32 hex digits, any case; odd lengths

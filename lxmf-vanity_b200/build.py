@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra"]
 
-CU_SOURCES = ["lxmfv.cu", "noalloc.cu"]
+CU_SOURCES = ["lxmfv.cu", "noalloc.cu", "pool.cu"]
 CXX_SOURCES = ["host.cpp"]
 HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "prim_kernels.cuh"]
 

@@ -77,7 +77,7 @@ __device__ __forceinline__ void to_affine(const fe& X, const fe& Y, const fe& Z,
 
 // The table: thread i computes i Q (i = 1..M) and thread 0 computes J = 2M Q,
 // affine and canonical, into tu / tv ([M + 1] each).
-__global__ void group_table_kernel(fe* tu, fe* tv, uint32_t m, fe q, fe vq) {
+static __global__ void group_table_kernel(fe* tu, fe* tv, uint32_t m, fe q, fe vq) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m) return;
     uint32_t s[8] = {i == 0 ? 2 * m : i, 0, 0, 0, 0, 0, 0, 0};
@@ -89,7 +89,7 @@ __global__ void group_table_kernel(fe* tu, fe* tv, uint32_t m, fe q, fe vq) {
 
 // Start from scalars: C = (k/8 + M) Q, the centre of the first group (walk
 // indices 0 .. 2M-1).
-__global__ void __launch_bounds__(128) group_start_kernel(uint32_t* state, uint64_t* ns,
+static __global__ void __launch_bounds__(128) group_start_kernel(uint32_t* state, uint64_t* ns,
                                                           const uint32_t* __restrict__ scalars, uint32_t lanes,
                                                           uint32_t m, fe q, fe vq) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) group_start_kernel(uint32_t* state, uint6
 
 // Start from Backend::init's u(k-8), u(k): y of P = kB = (k/8) Q is recovered
 // with -Q (P - Q is known, not P + Q), then C = P + T_M (tm = M Q).
-__global__ void __launch_bounds__(128) group_init_kernel(uint32_t* state, uint64_t* ns,
+static __global__ void __launch_bounds__(128) group_init_kernel(uint32_t* state, uint64_t* ns,
                                                          const uint32_t* __restrict__ upc, uint32_t lanes, fe q,
                                                          fe vq_neg, fe tmu, fe tmv) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
@@ -133,32 +133,27 @@ __global__ void __launch_bounds__(128) group_init_kernel(uint32_t* state, uint64
     ns[lane] = 0;
 }
 
+// `groups` groups of one lane's walk from centre (uc, vc) at walk index n
+// (the first key of the next group); emit(u, key) receives every key's
+// canonical u.  Shared by the plain walk and the pool's persistent kernel.
 // SYNC: a block barrier after each group keeps the block's warps in the same
 // phase of the walk, so that they share the instruction cache's working set
-// (one phase's code instead of all of it).  Threads past the last lane then
-// walk a copy of the last lane and neither emit nor store.
-template <int M, int BLOCK, int MINB, bool SYNC>
-__global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ GroupArgs<M> a) {
-    const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
-    if (!SYNC && tid >= a.lanes) return;
-    const bool active = tid < a.lanes;
-    const uint32_t lane = active ? tid : a.lanes - 1;
-    fe uc = load_fe(a.state, 0, lane, a.lanes);
-    fe vc = load_fe(a.state, 1, lane, a.lanes);
-    const uint64_t key0 = a.ns[lane];
-    uint64_t n = key0;
+// (one phase's code instead of all of it); every thread of the block must
+// then call this with the same `groups`.
+template <int M, bool SYNC, class Emit>
+__device__ __forceinline__ void walk_groups(fe& uc, fe& vc, uint64_t& n, uint32_t groups, const GroupTable<M>& t,
+                                            const Emit& emit) {
     fe pre[M + 1];
     fe cA = fe_zero();
     cA.v[0] = LXK_A;
-
 #pragma unroll 1
-    for (uint32_t it = 0; it < a.iters; ++it) {
+    for (uint32_t it = 0; it < groups; ++it) {
         // Denominators e_0 = u_J - u_C, e_i = u_{T_i} - u_C; pre[i] = e_0 ... e_{i-1}.
-        fe acc = fe_sub(a.t.u[0], uc);
+        fe acc = fe_sub(t.u[0], uc);
 #pragma unroll 1
         for (int i = 1; i <= M; ++i) {
             pre[i] = acc;
-            acc = fe_mul(acc, fe_sub(a.t.u[i], uc));
+            acc = fe_mul(acc, fe_sub(t.u[i], uc));
         }
         fe inv = fe_invert(acc);
         const uint64_t c = n + M;
@@ -166,7 +161,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_co
         fe vnext = vc;
 #pragma unroll 1
         for (int i = M; i >= 0; --i) {
-            const fe tu = a.t.u[i], tv = a.t.v[i];
+            const fe tu = t.u[i], tv = t.v[i];
             fe invi = inv;  // 1 / e_i
             if (i > 0) {
                 invi = fe_mul(inv, pre[i]);
@@ -189,7 +184,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_co
                 // side 1: key c - i (i = 0: the centre).
                 if (side == 1 || (i > 0 && i < M)) {
                     const fe u = fe_canon(side ? um : up);
-                    if (active) emit_key(a.em, lane, side ? c - (uint64_t)i : c + (uint64_t)i, key0, u);
+                    emit(u, side ? c - (uint64_t)i : c + (uint64_t)i);
                 }
             }
             if (i == 0) {
@@ -200,7 +195,33 @@ __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_co
         n += 2 * M;
         if (SYNC) __syncthreads();
     }
+}
 
+// The plain search's emission: one prefix for every lane of the launch.
+struct LaneEmit {
+    const EmitArgs& em;
+    uint32_t lane;
+    uint64_t key0;
+    bool active;
+    __device__ __forceinline__ void operator()(const fe& u, uint64_t key) const {
+        if (active) emit_key(em, lane, key, key0, u);
+    }
+};
+
+// Threads past the last lane walk a copy of the last lane and neither emit
+// nor store (with SYNC they must still reach every barrier).
+template <int M, int BLOCK, int MINB, bool SYNC>
+static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ GroupArgs<M> a) {
+    const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
+    if (!SYNC && tid >= a.lanes) return;
+    const bool active = tid < a.lanes;
+    const uint32_t lane = active ? tid : a.lanes - 1;
+    fe uc = load_fe(a.state, 0, lane, a.lanes);
+    fe vc = load_fe(a.state, 1, lane, a.lanes);
+    const uint64_t key0 = a.ns[lane];
+    uint64_t n = key0;
+    const LaneEmit emit{a.em, lane, key0, active};
+    walk_groups<M, SYNC>(uc, vc, n, a.iters, a.t, emit);
     if (active) {
         store_fe(a.state, 0, lane, a.lanes, uc);
         store_fe(a.state, 1, lane, a.lanes, vc);

@@ -35,7 +35,7 @@ __device__ __forceinline__ void store_words(uint32_t* p, const fe& x) {
     p4[1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
 }
 
-__global__ void fe_op_kernel(int op, const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+static __global__ void fe_op_kernel(int op, const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                              uint32_t* __restrict__ out, uint64_t count) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
         const fe x = load_words_drop255(a + 8 * i);
@@ -49,7 +49,7 @@ __global__ void fe_op_kernel(int op, const uint32_t* __restrict__ a, const uint3
 
 // Montgomery's trick over each group of `group` (<= 256) consecutive elements,
 // one group per thread; the structure of the walk's batch inversion.
-__global__ void fe_batch_invert_kernel(const uint32_t* __restrict__ a, uint32_t* __restrict__ out, uint64_t count,
+static __global__ void fe_batch_invert_kernel(const uint32_t* __restrict__ a, uint32_t* __restrict__ out, uint64_t count,
                                        uint32_t group) {
     const uint64_t groups = (count + group - 1) / group;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups; g += (uint64_t)gridDim.x * blockDim.x) {
@@ -71,7 +71,7 @@ __global__ void fe_batch_invert_kernel(const uint32_t* __restrict__ a, uint32_t*
 }
 
 // Destination hashes of whole 64-byte public keys (both halves per element).
-__global__ void address_chain_kernel(const uint32_t* __restrict__ pk, lxsha::AddrConsts ac, uint32_t* __restrict__ out,
+static __global__ void address_chain_kernel(const uint32_t* __restrict__ pk, lxsha::AddrConsts ac, uint32_t* __restrict__ out,
                                      uint64_t count) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t u[8], hi[8], d[4];
@@ -92,7 +92,7 @@ __global__ void address_chain_kernel(const uint32_t* __restrict__ pk, lxsha::Add
 // Operations counted per step and chain: kinds 2 and 5 issue two.
 //   0 mad.lo.u32   1 mad.hi.u32   2 xor + shf   3 mad.wide.u32 (64-bit addend)
 //   4 add.u32      5 mad.lo + xor (two pipes)   6 shf only   7 xor only
-__global__ void __launch_bounds__(256) probe_kernel(int kind, uint32_t iters, uint32_t seed, uint32_t* sink) {
+static __global__ void __launch_bounds__(256) probe_kernel(int kind, uint32_t iters, uint32_t seed, uint32_t* sink) {
     uint32_t x[8], y[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {

@@ -106,7 +106,7 @@ __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint6
 // phase (see group_walk_kernel); threads past the last lane then walk a copy
 // of the last lane and neither emit nor store.
 template <int B, int BLOCK, int MINB, bool SYNC>
-__global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant__ WalkArgs a) {
+static __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant__ WalkArgs a) {
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     if (!SYNC && tid >= a.lanes) return;
     const bool active = tid < a.lanes;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant
 
 // Backend::init (mod.rs:48): lane t from u(k-8), u(k) as 16 LE words, Z = 1.
 // Bit 255 of each u is dropped, as fe_from_words does (common.h:131-142).
-__global__ void init_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ upc, uint32_t lanes) {
+static __global__ void init_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ upc, uint32_t lanes) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     if (lane >= lanes) return;
     fe xp, xc;
@@ -231,7 +231,7 @@ __device__ __forceinline__ void scalar_over_8(const uint32_t* __restrict__ scala
 
 // x-only start: (P(-1), P(0)) = ((k-8)B, kB), left projective (replacing the
 // CPU start points of first_public_keys, mod.rs:212-228, for the walk).
-__global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ scalars,
+static __global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* ns, const uint32_t* __restrict__ scalars,
                                                      uint32_t lanes, fe q) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     if (lane >= lanes) return;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(128) ladder_kernel(uint32_t* state, uint64_t* 
 // first_public_keys (mod.rs:212-228) on the GPU: u(k-8) and u(k) as 16
 // canonical little-endian words per lane, the input of Backend::init.  One
 // inversion of Z2 * Z3 serves both coordinates.
-__global__ void __launch_bounds__(128) first_keys_kernel(uint32_t* __restrict__ upc, const uint32_t* __restrict__ scalars,
+static __global__ void __launch_bounds__(128) first_keys_kernel(uint32_t* __restrict__ upc, const uint32_t* __restrict__ scalars,
                                                          uint32_t lanes, fe q) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     if (lane >= lanes) return;

@@ -58,6 +58,26 @@ class Hit(C.Structure):
     _fields_ = [("thread", C.c_uint32), ("reserved", C.c_uint32), ("n", C.c_uint64)]
 
 
+class PoolOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("capacity_lanes", C.c_uint32), ("memory_budget", C.c_uint64),
+                ("batch", C.c_uint32), ("max_searches", C.c_uint32), ("max_hits", C.c_uint32),
+                ("stream", C.c_void_p)]
+
+
+class SearchDesc(C.Structure):
+    _fields_ = [("ed", C.c_uint32 * 8), ("name_hash", C.c_uint32 * 3), ("want", C.c_uint32 * 4),
+                ("mask", C.c_uint32 * 4), ("lanes", C.c_uint32)]
+
+
+class PoolHit(C.Structure):
+    _fields_ = [("search", C.c_uint32), ("lane", C.c_uint32), ("n", C.c_uint64)]
+
+
+class PoolInfo(C.Structure):
+    _fields_ = [("capacity_lanes", C.c_uint32), ("free_lanes", C.c_uint32), ("active_searches", C.c_uint32),
+                ("active_lanes", C.c_uint32), ("batch", C.c_uint32), ("sms", C.c_uint32)]
+
+
 _u8p = C.POINTER(C.c_uint8)
 _u32p = C.POINTER(C.c_uint32)
 _lib = None
@@ -96,6 +116,16 @@ SIGNATURES = {
     "lxmfv_peak_probe": ([C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_double)], C.c_int),
     "lxmfv_fe_batch_invert_static": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_char_p,
                                       C.c_size_t], C.c_int),
+    "lxmfv_pool_open": ([C.POINTER(PoolOptions), C.POINTER(C.c_void_p)], C.c_int),
+    "lxmfv_pool_last_error": ([C.c_void_p], C.c_char_p),
+    "lxmfv_pool_info": ([C.c_void_p, C.POINTER(PoolInfo)], C.c_int),
+    "lxmfv_pool_submit": ([C.c_void_p, C.POINTER(SearchDesc), _u8p, _u32p], C.c_int),
+    "lxmfv_pool_retire": ([C.c_void_p, C.c_uint32], C.c_int),
+    "lxmfv_pool_step": ([C.c_void_p, C.c_uint32], C.c_int),
+    "lxmfv_pool_poll": ([C.c_void_p, C.POINTER(PoolHit), C.c_uint32, _u32p], C.c_int),
+    "lxmfv_pool_keys_per_lane": ([C.c_void_p, C.c_uint32], C.c_uint64),
+    "lxmfv_pool_last_step_ms": ([C.c_void_p], C.c_float),
+    "lxmfv_pool_close": ([C.c_void_p], None),
 }
 STATIC_SCRATCH_ELEMS = 131072
 

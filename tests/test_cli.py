@@ -1,0 +1,99 @@
+"""The lxmf-vanity command line (the reference's CLI surface, src/main.rs:325-499).
+
+CPU tests cover argument handling and exit codes; GPU tests run real searches
+and the self-test, and check the written identity file from scratch with the
+oracle (address) and the file system (64 bytes, mode 0600, never overwritten)."""
+import os
+import re
+import stat
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "lxmf-vanity_b200", "lxmf-vanity")
+
+
+def run(args, cwd, timeout=300):
+    return subprocess.run([CLI] + args, cwd=cwd, capture_output=True, text=True, timeout=timeout)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    if not os.path.exists(CLI):
+        pytest.fail(f"{CLI} is not built (python lxmf-vanity_b200/build.py)")
+
+
+def test_usage_errors(tmp_path):
+    for args in ([], ["--gpu"], ["--bogus", "b0"], ["--cpu", "b0"], ["--gpu", "b0", "c1"], ["--walk", "slow", "--gpu", "b0"]):
+        r = run(args, tmp_path)
+        assert r.returncode == 1 and "usage:" in r.stderr, args
+
+
+def test_bad_prefix_is_refused(tmp_path):
+    r = run(["--gpu", "BOOB"], tmp_path)
+    assert r.returncode == 1
+    assert "isn't 1 to 32 hex digits" in r.stderr and "not the letter O" in r.stderr
+    r = run(["--gpu", "0" * 33], tmp_path)
+    assert r.returncode == 1
+
+
+def test_existing_identity_is_not_overwritten(tmp_path):
+    p = tmp_path / "b00.identity"
+    p.write_bytes(b"x" * 64)
+    r = run(["--gpu", "B00"], tmp_path)
+    assert r.returncode == 1 and "already exists; not overwriting it" in r.stderr
+    assert p.read_bytes() == b"x" * 64
+
+
+def test_no_gpu_reports_instead_of_crashing(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    r = run(["--gpu", "b0"], tmp_path)
+    assert r.returncode == 2 and "unavailable" in r.stderr
+    assert not (tmp_path / "b0.identity").exists()
+    r = run(["--gpu-self-test"], tmp_path)
+    assert r.returncode == 1 and "GPU unavailable" in r.stderr
+
+
+def _check_identity(path, prefix, aspect="lxmf.delivery"):
+    from oracle import oracle as O
+    data = path.read_bytes()
+    assert len(data) == 64
+    assert stat.S_IMODE(os.stat(path).st_mode) == 0o600
+    addr = O.address_of_identity(data, aspect)
+    assert O.prefix_matches(O.prefix_parse(prefix), addr)
+    return addr.hex()
+
+
+@pytest.mark.gpu
+def test_self_test_passes(tmp_path):
+    r = run(["--gpu-self-test"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    m = re.search(r"Self-test passed: (\d+) public keys match X25519, (\d+) hits", r.stdout)
+    assert m and int(m.group(1)) == 256 * 64 and int(m.group(2)) >= 100
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("walk", ["group", "xadd"])
+def test_search_writes_a_valid_identity(tmp_path, walk):
+    r = run(["--gpu", "--walk", walk, "B00B"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    addr = _check_identity(tmp_path / "b00b.identity", "b00b")
+    assert f"Found {addr}" in r.stdout
+    assert re.search(r"About \d+ tries in [\d.]+ s \(\d+/s\)\. Saved to b00b\.identity", r.stdout)
+    r = run(["--gpu", "b00b"], tmp_path)
+    assert r.returncode == 1 and "already exists" in r.stderr
+
+
+@pytest.mark.gpu
+def test_seeded_search_is_reproducible_and_honours_the_aspect(tmp_path):
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    for d in (a, b):
+        r = run(["--gpu", "--seed", "12345", "--aspect", "nomadnetwork.node", "--lanes", "8192", "abc"], d)
+        assert r.returncode == 0, r.stderr
+    assert (a / "abc.identity").read_bytes() == (b / "abc.identity").read_bytes()
+    _check_identity(a / "abc.identity", "abc", "nomadnetwork.node")

@@ -1,0 +1,106 @@
+"""The search pool (many searches in one persistent kernel), the batched
+runner and the serving loop, through the C ABI.
+
+Bit-exact: every hit of every search against the oracle's search over the
+same lanes and keys; a search's hits are the same alone and in a mix of 64
+others (same lanes, same steps); admission stops at the pool's capacity and
+resumes after a retirement, with the remaining searches walking on."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def srv():
+    import lxmfv_serve
+    return lxmfv_serve
+
+
+def _oracle_hits(oracle, spec, keys):
+    nh = oracle.name_hash(spec.aspect)
+    ed_pub = oracle.ed25519_public(spec.ed_seed)
+    pfx = oracle.prefix_parse(spec.prefix)
+    out = set()
+    for lane in range(spec.lanes):
+        h, _ = oracle.search_window(bytes(spec.scalars[lane]), ed_pub, nh, pfx, keys)
+        out.update((lane, int(n)) for n in h)
+    return out
+
+
+@pytest.mark.parametrize("batch", [64, 256])
+def test_pool_hits_match_oracle(srv, oracle, batch):
+    specs = [srv.SearchSpec.seeded(11, "b0", "lxmf.delivery", 96),
+             srv.SearchSpec.seeded(12, "7", "nomadnetwork.node", 64),
+             srv.SearchSpec.seeded(13, "c3", "lxmf.propagation", 160)]
+    with srv.Pool(device=0, capacity_lanes=4096, batch=batch) as pool:
+        sids = [pool.submit(s) for s in specs]
+        pool.step(1)
+        pool.step(1)
+        hits, n = pool.poll()
+        assert n == len(hits)
+        for sid, spec in zip(sids, specs):
+            got = {(lane, k) for s, lane, k in hits if s == sid}
+            assert got == _oracle_hits(oracle, spec, 2 * batch), spec.prefix
+            assert pool.keys_per_lane(sid) == 2 * batch
+
+
+def test_a_search_is_the_same_alone_and_in_a_mix(srv):
+    target = srv.SearchSpec.seeded(777, "a5", "lxmf.delivery", 512)
+    others = srv.batched_specs(64, seed=5, lanes=512, min_nibbles=2, max_nibbles=6)
+
+    def hits_of(mix):
+        with srv.Pool(device=0, capacity_lanes=65 * 512, batch=256) as pool:
+            ids = [pool.submit(s) for s in mix]
+            sid = ids[0]
+            got = set()
+            for _ in range(3):
+                pool.step(2)
+                h, _ = pool.poll()
+                got.update((lane, n) for s, lane, n in h if s == sid)
+            return got
+
+    alone = hits_of([target])
+    mixed = hits_of([target] + others)
+    assert alone == mixed and len(alone) > 50
+
+
+def test_admission_retirement_and_continuity(srv, oracle):
+    a = srv.SearchSpec.seeded(21, "e", "lxmf.delivery", 64)
+    b = srv.SearchSpec.seeded(22, "4", "lxmf.delivery", 64)
+    c = srv.SearchSpec.seeded(23, "9", "nomadnetwork.node", 64)
+    with srv.Pool(device=0, capacity_lanes=128, batch=64) as pool:
+        sa = pool.submit(a)
+        sb = pool.submit(b)
+        with pytest.raises(Exception) as e:
+            pool.submit(c)
+        assert "free" in str(e.value)
+        info = pool.info()
+        assert info["free_lanes"] == 0 and info["active_searches"] == 2
+        pool.step(1)
+        pool.poll()
+        pool.retire(sb)
+        sc = pool.submit(c)
+        pool.step(1)
+        hits, _ = pool.poll()
+        got_a = {(lane, n) for s, lane, n in hits if s == sa}
+        got_c = {(lane, n) for s, lane, n in hits if s == sc}
+        exp_a = {(lane, n) for lane, n in _oracle_hits(oracle, a, 128) if n >= 64}
+        assert got_a == exp_a  # a walked on from where it was
+        assert got_c == _oracle_hits(oracle, c, 64)  # c started from its own keys in b's old lanes
+        assert pool.keys_per_lane(sa) == 128 and pool.keys_per_lane(sc) == 64
+
+
+def test_batched_runner_rechecks(srv):
+    specs = srv.batched_specs(32, seed=9, lanes=256, min_nibbles=2, max_nibbles=5)
+    with srv.Pool(device=0, capacity_lanes=32 * 256, batch=128) as pool:
+        r = srv.run_batched(pool, specs, steps=2, groups=1, recheck_limit=8)
+    assert r["rechecked_bad"] == 0 and r["hits_rechecked"] > 20 and r["keys_per_s"] > 0
+
+
+def test_serving_loop_finishes_every_request(srv):
+    reqs = srv.poisson_requests(rate=40.0, duration=1.0, seed=3, lanes=256, min_nibbles=2, max_nibbles=4, p=0.6)
+    with srv.Pool(device=0, capacity_lanes=8 * 256, batch=64) as pool:
+        out = srv.serve(pool, reqs, groups=1, time_limit=120)
+    assert out["done"] == len(reqs) and out["rechecked_bad"] == 0
+    assert all(r.tries > 0 and r.walked >= r.tries for r in reqs)

@@ -36,6 +36,30 @@ def test_open_reports_errors_instead_of_aborting(lx):
     assert e.value.code == lx.ERR_CUDA and "CUDA" in str(e.value)
 
 
+def test_pool_open_reports_errors(lx):
+    import torch
+
+    import lxmfv_serve
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(lx.LxmfvError) as e:
+        lxmfv_serve.Pool(device=0)
+    assert e.value.code == lx.ERR_CUDA
+    with pytest.raises(lx.LxmfvError) as e:
+        lxmfv_serve.Pool(device=0, batch=100)
+    assert e.value.code == lx.ERR_ARG
+
+
+def test_served_request_stream_is_seeded(lx):
+    import lxmfv_serve
+    a = lxmfv_serve.poisson_requests(50.0, 2.0, seed=4, lanes=32)
+    b = lxmfv_serve.poisson_requests(50.0, 2.0, seed=4, lanes=32)
+    assert [(r.arrival, r.spec.prefix, r.spec.aspect) for r in a] == [(r.arrival, r.spec.prefix, r.spec.aspect) for r in b]
+    assert 60 < len(a) < 140
+    assert all(5 <= r.spec.nibbles <= 9 for r in a)
+    assert all(r.spec.aspect in lxmfv_serve.ASPECTS for r in a)
+
+
 def test_bad_options_are_rejected(lx):
     with pytest.raises(lx.LxmfvError) as e:
         lx.Backend(batch=48)
