@@ -72,6 +72,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
     p.add_argument("--no-b64", action="store_true", help="skip the second measurement at B = 64")
+    p.add_argument("--no-batched", action="store_true", help="skip the 256-search batched measurement")
+    p.add_argument("--served-seconds", type=float, default=20.0,
+                   help="length of the served-requests run (0: skip); the full served workload is 600")
     return p.parse_args()
 
 
@@ -216,6 +219,37 @@ def reference_cuda_kernel(b, lx, prefix: str) -> dict | None:
             "build": "reference src/gpu/kernel.cu + common.h, nvcc -gencode arch=compute_100a,code=sm_100a -O3"}
 
 
+def batched_workload(lx, dev: int, single_value: float) -> dict:
+    """256 concurrent searches in the pool's persistent kernel: prefix lengths
+    uniform over 4-10 nibbles with random hex, aspects uniform over three, each
+    with its own seeded identity; 1184 lanes each, so that the persistent
+    kernel's work items (512 lanes) are exactly 4 per SM; G = 256, 4 groups per
+    step (the autotuned setting); aggregate device keys/s against the single
+    search's `value`."""
+    import lxmfv_serve as srv
+    specs = srv.batched_specs(256, seed=4, lanes=1184, min_nibbles=4, max_nibbles=10)
+    with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=256) as pool:
+        r = srv.run_batched(pool, specs, steps=6, groups=4, warmup=1, recheck_limit=8)
+    r["vs_single_search"] = r["keys_per_s"] / single_value
+    r["workload"] = "256 searches, 4-10 nibbles, 3 aspects, 1184 lanes each, one persistent launch per step"
+    return r
+
+
+def served_workload(dev: int, seconds: float) -> dict:
+    """Served requests: Poisson arrivals at 50 per second for `seconds`, prefix
+    length 5 + Geometric(0.9) - 1 truncated to 5-9 nibbles, random hex, aspects
+    as in the batched workload, seeded identities; lanes by difficulty
+    (64 x 16^(L-5), at most 32768); a pool of 262144 lanes (28 MB of walker
+    state) as the memory budget; every search retired on its first hit."""
+    import lxmfv_serve as srv
+    reqs = srv.poisson_requests(rate=50.0, duration=seconds, seed=8, lanes=srv.lanes_by_difficulty)
+    with srv.Pool(device=dev, capacity_lanes=262144, batch=256) as pool:
+        out = srv.serve(pool, reqs, groups=1, time_limit=seconds + 240)
+    out["workload"] = (f"Poisson 50 req/s for {seconds:.0f} s, 5-9 nibbles (geometric p=0.9), lanes by difficulty, "
+                       "262144-lane pool")
+    return out
+
+
 def main() -> None:
     a = parse()
     world, rank, local = dist_setup()
@@ -265,6 +299,10 @@ def main() -> None:
                       a.warmup, e2e=False)
         line["at_batch_64"] = {"value": b64["value"], "unit": "keys/s", "ms_per_step": b64["ms_per_step"],
                                "config": b64["config"], "clocks": b64["clocks"], "hits": b64["hits"]}
+    if rank == 0 and world == 1 and not a.no_batched:
+        line["batched"] = batched_workload(lx, dev, head["value"])
+    if rank == 0 and world == 1 and a.served_seconds > 0:
+        line["served"] = served_workload(dev, a.served_seconds)
     if rank == 0 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prefix)
     if rank == 0 and not a.no_ref_cuda:

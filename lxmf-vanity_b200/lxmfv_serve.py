@@ -237,11 +237,19 @@ class Request:
     hit: tuple[int, int] | None = None  # (lane, n)
 
 
-def poisson_requests(rate: float, duration: float, seed: int, lanes: int, min_nibbles: int = 5,
+def lanes_by_difficulty(nibbles: int, base: int = 64, cap: int = 32768) -> int:
+    """Lanes for a request: 64 for 5 nibbles, 16 times more per further nibble,
+    at most `cap`, so that expected steps to a hit stay about level."""
+    return int(min(cap, max(32, base * 16 ** max(0, nibbles - 5))))
+
+
+def poisson_requests(rate: float, duration: float, seed: int, lanes, min_nibbles: int = 5,
                      max_nibbles: int = 9, p: float = 0.9) -> list[Request]:
-    """Arrivals of a Poisson stream; prefix length 5 + Geometric(p) truncated to
-    [min, max] nibbles, random hex; aspects uniform over three; seeded identities."""
+    """Arrivals of a Poisson stream; prefix length min + Geometric(p) - 1,
+    redrawn above max (a truncated geometric); random hex; aspects uniform over
+    three; seeded identities.  `lanes` is a count or a function of nibbles."""
     rng = np.random.default_rng(seed)
+    lanes_of = lanes if callable(lanes) else (lambda _n, k=lanes: k)
     t, reqs = 0.0, []
     while True:
         t += float(rng.exponential(1.0 / rate))
@@ -253,7 +261,7 @@ def poisson_requests(rate: float, duration: float, seed: int, lanes: int, min_ni
                 break
         prefix = "".join("0123456789abcdef"[x] for x in rng.integers(0, 16, nib))
         aspect = ASPECTS[int(rng.integers(0, len(ASPECTS)))]
-        reqs.append(Request(t, SearchSpec.seeded(seed * 1000003 + len(reqs), prefix, aspect, lanes)))
+        reqs.append(Request(t, SearchSpec.seeded(seed * 1000003 + len(reqs), prefix, aspect, lanes_of(nib))))
     return reqs
 
 
