@@ -50,6 +50,15 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
     return (5 * m + 13) / b, (2 * m + 255) / b
 
 
+# Per key, from one ncu capture of each kernel (profiles/walk_group_g256_plain_search.md,
+# profiles/walk_xadd_b128_plain_search.md): ALU-pipe lane operations (the binding pipe),
+# all instructions, and DRAM bytes (read + write).
+NCU_PER_KEY = {
+    ("group", 256): {"alu": 3352, "inst": 5878, "dram_bytes": 28.6},
+    ("xadd", 128): {"alu": 4308, "inst": 7909, "dram_bytes": 119.4},
+}
+
+
 def wide_products_per_key(walk: str, b: int) -> float:
     """32x32->64 products per key with 8 x 32-bit limbs: a field multiply is
     64 + 8 (the fold by 38), a square 36 + 8."""
@@ -390,12 +399,26 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
     kernel_s = ms * 1e-3 / steps
     mul, sqr = field_ops_per_key(walk, batch)
     prods = wide_products_per_key(walk, batch)
-    achieved = 2 * prods * keys_per_step / kernel_s  # lo + hi IMAD per 32x32->64 product
-    roofline = {"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
-                "frac": achieved / imad_peak, "traffic": None,
-                "note": f"algorithmic {mul:.2f} M + {sqr:.2f} S = {prods:.0f} 32x32->64 products "
-                        f"(lo + hi IMAD each) per key; peak = measured mad.lo.u32 rate of this GPU (probe)",
-                "alu_peak": alu_peak / 1e12}
+    keys_per_s_kernel = keys_per_step / kernel_s
+    imad = 2 * prods * keys_per_s_kernel  # lo + hi IMAD per 32x32->64 product
+    imad_line = {"achieved": imad / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s", "frac": imad / imad_peak,
+                 "note": f"algorithmic {mul:.2f} M + {sqr:.2f} S = {prods:.0f} 32x32->64 products (lo + hi IMAD "
+                         f"each) per key; peak = measured mad.lo.u32 rate of this GPU (probe)"}
+    ncu = NCU_PER_KEY.get((walk, batch))
+    if ncu:
+        # The binding resource: the integer ALU pipe (SHA-256 rotates and LOP3s, carry handling).
+        alu = ncu["alu"] * keys_per_s_kernel
+        issue_peak = 2 * alu_peak  # 4 warp-instructions per SM per clock: twice the ALU pipe's lane rate
+        roofline = {"bound": "alu", "achieved": alu / 1e12, "peak": alu_peak / 1e12, "unit": "T ALU lane-ops/s",
+                    "frac": alu / alu_peak, "traffic": ncu["dram_bytes"] * keys_per_step,
+                    "note": f"{ncu['alu']} ALU-pipe lane-ops per key (ncu, profiles/) x keys/s over the measured "
+                            f"xor + funnel-shift rate of this GPU (probe); traffic = ncu DRAM bytes per key x keys "
+                            f"per launch",
+                    "issue": {"achieved": ncu["inst"] * keys_per_s_kernel / 1e12, "peak": issue_peak / 1e12,
+                              "unit": "T inst/s", "frac": ncu["inst"] * keys_per_s_kernel / issue_peak},
+                    "imad": imad_line}
+    else:
+        roofline = dict(imad_line, bound="imad", traffic=None, alu_peak=alu_peak / 1e12)
     config = {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, seeded walkers, 2^36 keys per run)",
               "walk": walk, "prefix": prefix, "lanes_per_gpu": lanes, "batch": batch, "iters_per_step": iters,
               "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
