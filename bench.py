@@ -16,7 +16,8 @@ launching stream, max over ranks), `e2e` goes through the C ABI's
 synchronous lxmfv_launch with host buffers, `cpu_baseline` is the restated
 CPU search on this host's cores, `roofline` relates the walk kernel's
 multiply work to the measured IMAD rate of this GPU, and
-`reference_cuda_kernel` times the reference's own CUDA kernel on this GPU.
+`reference_cuda_kernel` times the reference's own CUDA kernel on this GPU and
+`cpu_search` this library's CPU search (the reference's default mode).
 With --impl reference, the reference's own kernel body (src/gpu/common.h,
 built for the host) is timed on the host cores instead.
 """
@@ -78,6 +79,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--block", type=int, default=0)
     p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cpu-search", action="store_true", help="skip timing this library's CPU search")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
     p.add_argument("--no-b64", action="store_true", help="skip the second measurement at B = 64")
@@ -154,6 +156,25 @@ def cpu_baseline_port(prefix: str, seconds: float = 2.5) -> dict:
     return {"value": rate, "unit": "keys/s", "cores": threads, "kind": "port",
             "sample": f"{keys} keys: {threads} threads x {per_thread} keys each from seeded starts, "
                       f"prefix {prefix}, restated KeyWalk (B=256) + double SHA-256 per key"}
+
+
+def cpu_search_rate(seconds: float = 3.0) -> dict:
+    """This library's own CPU search (lxmfv_cpu_search: the reference's
+    default mode) on every host core for `seconds`, with a prefix it will not
+    find in that time."""
+    import threading
+
+    import lxmfv as lx
+    threads = os.cpu_count() or 1
+    s = lx.CpuSearch(lx.prefix_parse("0123456789abcdef"), threads=threads, seed=SEED)
+    timer = threading.Timer(seconds, s.stop)
+    t0 = time.perf_counter()
+    timer.start()
+    found = s.run()
+    dt = time.perf_counter() - t0
+    return {"value": s.tries / dt, "unit": "keys/s", "threads": threads, "seconds": round(dt, 2),
+            "found": found is not None,
+            "api": "lxmfv_cpu_search (x-only walk, 5 x 51-bit field, x86 SHA extensions where present)"}
 
 
 def reference_cpu(prefix: str, steps: int, warmup: int, step_seconds: float = 2.0) -> dict:
@@ -314,6 +335,8 @@ def main() -> None:
         line["served"] = served_workload(dev, a.served_seconds)
     if rank == 0 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prefix)
+    if rank == 0 and not a.no_cpu_search:
+        line["cpu_search"] = cpu_search_rate()
     if rank == 0 and not a.no_ref_cuda:
         with lx.Backend(device=dev, lanes=1024) as b:
             line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)

@@ -279,6 +279,37 @@ int lxmfv_x25519_base(const uint8_t k[32], uint8_t out[32]);
  * an independent implementation (OpenSSL): the recheck every hit passes. */
 int lxmfv_address_of_identity(const uint8_t identity[64], const uint8_t name_hash[10], uint8_t out[16]);
 
+/* ---- The CPU search (the reference's default mode and the CPU half of
+ * --gpu --cpu).  Runs only when called; no GPU entry point falls back to it. */
+
+/* lxmfv_cpu_search found no hit before *stop became nonzero. */
+#define LXMFV_STOPPED 1
+#define LXMFV_CPU_MAX_THREADS 4096
+
+/* lxmf_address (main.rs:180-189) on `count` 64-byte public keys (x_pub then
+ * ed_pub) with one name hash, on this CPU thread: 16-byte outputs.  impl 0:
+ * the SHA-256 the CPU search uses (the x86 SHA extensions where present);
+ * 1: portable C; 2: the SHA extensions (LXMFV_ERR_STATE where absent). */
+int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out, int impl);
+
+/* KeyWalk::next_batch (main.rs:255-289) from start scalar k: writes the
+ * X25519 public keys u(k + 8n), n = 0 .. count-1, 32 bytes each. */
+int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys);
+
+/* search on `threads` CPU threads (main.rs:292-323, fanned out as
+ * run_search, main.rs:360-432) until one finds an address starting with the
+ * prefix, or until *stop (read atomically) becomes nonzero.  seed NULL: each
+ * thread draws its own start scalar and Ed25519 seed from the OS, as the
+ * reference.  seed given: thread t walks seeded walker first_walker + t
+ * (walker 0 = the seeded identity's scalar, walker w = the w-th further
+ * scalar draw, first_walker <= 2^24) with the identity's Ed25519 seed.
+ * *tries (may be NULL) is updated every 10 ms with the keys tried.  Writes
+ * the rechecked 64-byte identity and returns LXMFV_OK; LXMFV_STOPPED when
+ * stopped without a hit; LXMFV_ERR_RECHECK when a hit failed its recheck. */
+int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
+                     const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
+                     uint8_t identity[64]);
+
 /* ---- Primitive kernels (the field and hash microbench). ---- */
 
 /* Field op on `count` elements of 8 little-endian words on the GPU: inputs

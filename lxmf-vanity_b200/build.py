@@ -26,8 +26,9 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xco
 CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra"]
 
 CU_SOURCES = ["lxmfv.cu", "noalloc.cu", "pool.cu"]
-CXX_SOURCES = ["host.cpp"]
-HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "prim_kernels.cuh"]
+CXX_SOURCES = ["host.cpp", "cpu_search.cpp"]
+HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "prim_kernels.cuh",
+           "cpu_sha256.h"]
 
 
 def _run(cmd: list[str], verbose: bool) -> str:

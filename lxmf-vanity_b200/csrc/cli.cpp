@@ -1,7 +1,9 @@
 // lxmf-vanity: the reference's command line (src/main.rs:325-499) over the
 // B200 library.
 //
-//   lxmf-vanity --gpu <hex prefix>        search on the GPU(s); writes <prefix>.identity
+//   lxmf-vanity <hex prefix>              search on every CPU core; writes <prefix>.identity
+//   lxmf-vanity --gpu <hex prefix>        search on the GPU(s)
+//   lxmf-vanity --gpu --cpu <hex prefix>  the GPU(s) and the remaining CPU cores together
 //   lxmf-vanity --gpu-self-test           check the GPU against the CPU
 //
 // Kept from the reference: the prefix rules (Prefix::parse, main.rs:206-216),
@@ -9,16 +11,19 @@
 // created new with mode 0600 (main.rs:484-493), the progress line every 10 s
 // (main.rs:407-421), the "Found" / "About" lines (main.rs:495-498, also read by
 // fleet.sh), launches grown towards 500 ms (mod.rs:148-174), every hit rebuilt
-// and rechecked from scratch on the CPU before it is accepted (mod.rs:156-160)
-// and the self-test (mod.rs:178-207).
+// and rechecked from scratch on the CPU before it is accepted (mod.rs:156-160),
+// the self-test (mod.rs:178-207) and the three modes with their thread
+// counts: every core; the GPU alone; the GPU and every core but one
+// (main.rs:473-480).
 // Added: --aspect (the destination aspect; default lxmf.delivery), --seed
 // (seeded walkers and identity instead of OS randomness), --devices (one
 // host thread per GPU, first hit wins: fleet.sh's mode in one process),
-// --walk / --batch / --lanes (kernel choice).
+// --threads (CPU threads), --walk / --batch / --lanes (kernel choice).
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cctype>
 #include <cerrno>
@@ -37,18 +42,22 @@
 namespace {
 
 const char* USAGE =
-    "usage: lxmf-vanity --gpu [options] <hex prefix>\n"
+    "usage: lxmf-vanity [--gpu [--cpu]] [options] <hex prefix>\n"
     "       lxmf-vanity --gpu-self-test [options]\n"
     "\n"
     "Finds a Reticulum identity whose LXMF address starts with the prefix and\n"
     "saves it to <prefix>.identity (readable only by you).\n"
     "\n"
+    "  (no flag)          search on every CPU core\n"
     "  --gpu              search on the GPU (NVIDIA B200)\n"
+    "  --gpu --cpu        search on the GPU and the remaining CPU cores together\n"
     "  --gpu-self-test    check the GPU's results against the CPU\n"
     "options:\n"
     "  --aspect NAME      destination aspect (default lxmf.delivery)\n"
     "  --devices LIST     GPUs to search on, e.g. 0,1,2,3 (default 0); first hit wins\n"
-    "  --seed N           seeded walkers and identity (ChaCha20 stream of N) instead of OS randomness\n"
+    "  --threads N        CPU threads (default: every core; with --gpu, every core but one)\n"
+    "  --seed N           seeded walkers and identity (ChaCha20 stream of N) instead of OS randomness;\n"
+    "                     GPU d uses seed N + d, the CPU threads seed N + (number of GPUs)\n"
     "  --walk group|xadd  the walk (default group; xadd is the x-only differential walk)\n"
     "  --batch N          keys per inversion (default 64)\n"
     "  --lanes N          walker lanes per GPU (default: one full wave)";
@@ -63,6 +72,7 @@ struct Options {
     bool seeded = false;
     uint64_t seed = 0;
     uint32_t walk = LXMFV_WALK_GROUP, batch = 64, lanes = 0;
+    int threads = 0;  // CPU threads; 0: the mode's default
 };
 
 struct Prefix {
@@ -163,6 +173,8 @@ struct GpuSearch {
 struct Shared {
     std::atomic<bool> found{false};
     std::atomic<uint64_t> tries{0};
+    uint64_t cpu_tries = 0;  // written by lxmfv_cpu_search, read atomically
+    int cpu_stop = 0;        // read by lxmfv_cpu_search, written atomically
     std::mutex mu;
     bool have_hit = false;
     uint8_t hit[64];
@@ -227,6 +239,28 @@ void run_device(const Options& o, const Prefix& p, int device, Shared& sh) {
         // Grow launches towards about 500 ms.
         if (took < 0.25 && iters < (1u << 16)) iters *= 2;
     }
+}
+
+// The CPU half: search (main.rs:292-323) on `threads` threads until a hit here
+// or elsewhere.
+void run_cpu(const Options& o, const Prefix& p, int threads, Shared& sh) {
+    uint8_t nh[10], ident[64];
+    lxmfv_name_hash(o.aspect.c_str(), nh);
+    const uint64_t seed = o.seed + (o.gpu ? (uint64_t)o.devices.size() : 0);
+    const int rc = lxmfv_cpu_search(p.bytes, p.nibbles, nh, threads, o.seeded ? &seed : nullptr, 0, &sh.cpu_stop,
+                                    &sh.cpu_tries, ident);
+    if (rc == LXMFV_STOPPED) return;
+    std::lock_guard<std::mutex> l(sh.mu);
+    if (rc == LXMFV_OK) {
+        if (!sh.have_hit) {
+            memcpy(sh.hit, ident, 64);
+            sh.have_hit = true;
+        }
+    } else if (sh.error.empty()) {
+        sh.error = rc == LXMFV_ERR_RECHECK ? "internal error: a CPU hit failed its recheck; not saving it"
+                                           : "CPU search failed (code " + std::to_string(rc) + ")";
+    }
+    sh.found = true;
 }
 
 int self_test(const Options& o) {
@@ -325,6 +359,7 @@ int main(int argc, char** argv) {
         else if (a == "--walk" && value(v) && (v == "group" || v == "xadd")) o.walk = v == "group" ? LXMFV_WALK_GROUP : LXMFV_WALK_XADD;
         else if (a == "--batch" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n < 4096) o.batch = (uint32_t)n;
         else if (a == "--lanes" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n < (1ull << 31)) o.lanes = (uint32_t)n;
+        else if (a == "--threads" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n <= LXMFV_CPU_MAX_THREADS) o.threads = (int)n;
         else if (a.rfind("--", 0) == 0) {
             fprintf(stderr, "%s\n", USAGE);
             return 1;
@@ -335,15 +370,8 @@ int main(int argc, char** argv) {
         return 1;
     }
     if (o.self_test) return self_test(o);
-    if (words.size() != 1 || !o.gpu) {
-        if (words.size() == 1 && !o.gpu)
-            fprintf(stderr, "This build searches on the GPU: use --gpu.\n");
-        else
-            fprintf(stderr, "%s\n", USAGE);
-        return 1;
-    }
-    if (o.cpu) {
-        fprintf(stderr, "--cpu: this build searches on the GPU only; use --gpu alone.\n");
+    if (words.size() != 1) {
+        fprintf(stderr, "%s\n", USAGE);
         return 1;
     }
     Prefix p;
@@ -363,19 +391,30 @@ int main(int argc, char** argv) {
     }
     printf("Looking for an LXMF address starting %s.\n", text.c_str());
     const double expected = std::pow(16.0, p.nibbles);
-    printf("Searching on %zu GPU%s; about %.0f tries on average.\n", o.devices.size(), o.devices.size() > 1 ? "s" : "",
-           expected);
+    // Every core; with the GPU, one core per GPU is left to drive it (main.rs:473-480).
+    const int cores = (int)std::max(1u, std::thread::hardware_concurrency());
+    int cpu_threads = o.threads;
+    if (!cpu_threads) cpu_threads = !o.gpu ? cores : o.cpu ? std::max(1, cores - (int)o.devices.size()) : 0;
+    if (o.gpu && !o.cpu) cpu_threads = 0;
+    std::string on;
+    if (o.gpu) on = std::to_string(o.devices.size()) + (o.devices.size() > 1 ? " GPUs" : " GPU");
+    if (cpu_threads)
+        on += (on.empty() ? "" : " and ") + std::to_string(cpu_threads) + (cpu_threads > 1 ? " CPU threads" : " CPU thread");
+    printf("Searching on %s; about %.0f tries on average.\n", on.c_str(), expected);
     fflush(stdout);
 
     Shared sh;
     const auto start = Clock::now();
     std::vector<std::thread> threads;
-    for (int d : o.devices) threads.emplace_back(run_device, std::cref(o), std::cref(p), d, std::ref(sh));
+    if (o.gpu)
+        for (int d : o.devices) threads.emplace_back(run_device, std::cref(o), std::cref(p), d, std::ref(sh));
+    if (cpu_threads) threads.emplace_back(run_cpu, std::cref(o), std::cref(p), cpu_threads, std::ref(sh));
+    auto all_tries = [&sh]() { return sh.tries.load() + __atomic_load_n(&sh.cpu_tries, __ATOMIC_RELAXED); };
     auto next_report = start + std::chrono::seconds(10);
     while (!sh.found.load()) {
         std::this_thread::sleep_for(std::chrono::milliseconds(50));
         if (Clock::now() >= next_report) {
-            const double done = (double)sh.tries.load();
+            const double done = (double)all_tries();
             const double rate = done / std::chrono::duration<double>(Clock::now() - start).count();
             if (done < expected)
                 printf("%.0f tries, %.0f/s; the average is about %.0f min away\n", done, rate,
@@ -386,6 +425,7 @@ int main(int argc, char** argv) {
             next_report += std::chrono::seconds(10);
         }
     }
+    __atomic_store_n(&sh.cpu_stop, 1, __ATOMIC_RELAXED);
     for (auto& t : threads) t.join();
     if (!sh.error.empty() && !sh.have_hit) {
         fprintf(stderr, "%s\n", sh.error.c_str());
@@ -405,7 +445,7 @@ int main(int argc, char** argv) {
     uint8_t addr[16], nh[10];
     lxmfv_name_hash(o.aspect.c_str(), nh);
     lxmfv_address_of_identity(sh.hit, nh, addr);
-    const uint64_t tried = sh.tries.load();
+    const uint64_t tried = all_tries();
     printf("Found %s\n", hex(addr, 16).c_str());
     printf("About %llu tries in %.1f s (%.0f/s). Saved to %s\n", (unsigned long long)tried, elapsed,
            (double)tried / elapsed, path.c_str());

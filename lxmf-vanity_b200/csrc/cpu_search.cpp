@@ -1,0 +1,343 @@
+// The CPU search: the reference's `lxmf-vanity <prefix>` mode and the CPU half
+// of `--gpu --cpu` (search and KeyWalk, src/main.rs:230-323; run_search's
+// thread fan-out, main.rs:360-432).  It runs only when a caller asks for a CPU
+// search; the GPU entry points never fall back to it.
+//
+// Per thread, as the reference: one start scalar k and one Ed25519 seed; the
+// X25519 keys u(k + 8n) by x-only differential addition of Q = 8B, 256 at a
+// time with their Z coordinates inverted together (Montgomery's trick); each
+// key's address by the double SHA-256 (cpu_sha256.h: the x86 SHA extensions
+// where present); a hit is rebuilt from its scalar and rechecked from scratch
+// (OpenSSL) before it is returned.
+// Field: GF(2^255-19) in 5 x 51-bit limbs with 128-bit products.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../../include/lxmfv.h"
+#include "cpu_sha256.h"
+
+namespace {
+
+typedef unsigned __int128 u128;
+constexpr uint64_t MASK51 = (1ull << 51) - 1;
+constexpr int BATCH = 256;  // keys per inversion, as main.rs's BATCH
+
+struct F {
+    uint64_t l[5];
+};
+
+const F ONE = {{1, 0, 0, 0, 0}};
+
+inline F carry(F a) {
+    for (int i = 0; i < 4; i++) {
+        a.l[i + 1] += a.l[i] >> 51;
+        a.l[i] &= MASK51;
+    }
+    a.l[0] += 19 * (a.l[4] >> 51);
+    a.l[4] &= MASK51;
+    a.l[1] += a.l[0] >> 51;
+    a.l[0] &= MASK51;
+    return a;
+}
+
+inline F add(const F& a, const F& b) {
+    F r;
+    for (int i = 0; i < 5; i++) r.l[i] = a.l[i] + b.l[i];
+    return carry(r);
+}
+
+// a - b + 4p: the limbs of a carried value stay below 2^52, 4p's are above.
+inline F sub(const F& a, const F& b) {
+    F r;
+    r.l[0] = a.l[0] + 4 * (MASK51 - 18) - b.l[0];
+    for (int i = 1; i < 5; i++) r.l[i] = a.l[i] + 4 * MASK51 - b.l[i];
+    return carry(r);
+}
+
+inline F mul(const F& a, const F& b) {
+    const uint64_t b1 = 19 * b.l[1], b2 = 19 * b.l[2], b3 = 19 * b.l[3], b4 = 19 * b.l[4];
+    u128 t0 = (u128)a.l[0] * b.l[0] + (u128)a.l[1] * b4 + (u128)a.l[2] * b3 + (u128)a.l[3] * b2 + (u128)a.l[4] * b1;
+    u128 t1 = (u128)a.l[0] * b.l[1] + (u128)a.l[1] * b.l[0] + (u128)a.l[2] * b4 + (u128)a.l[3] * b3 + (u128)a.l[4] * b2;
+    u128 t2 = (u128)a.l[0] * b.l[2] + (u128)a.l[1] * b.l[1] + (u128)a.l[2] * b.l[0] + (u128)a.l[3] * b4 + (u128)a.l[4] * b3;
+    u128 t3 = (u128)a.l[0] * b.l[3] + (u128)a.l[1] * b.l[2] + (u128)a.l[2] * b.l[1] + (u128)a.l[3] * b.l[0] + (u128)a.l[4] * b4;
+    u128 t4 = (u128)a.l[0] * b.l[4] + (u128)a.l[1] * b.l[3] + (u128)a.l[2] * b.l[2] + (u128)a.l[3] * b.l[1] + (u128)a.l[4] * b.l[0];
+    F r;
+    t1 += (uint64_t)(t0 >> 51);
+    r.l[0] = (uint64_t)t0 & MASK51;
+    t2 += (uint64_t)(t1 >> 51);
+    r.l[1] = (uint64_t)t1 & MASK51;
+    t3 += (uint64_t)(t2 >> 51);
+    r.l[2] = (uint64_t)t2 & MASK51;
+    t4 += (uint64_t)(t3 >> 51);
+    r.l[3] = (uint64_t)t3 & MASK51;
+    r.l[4] = (uint64_t)t4 & MASK51;
+    r.l[0] += 19 * (uint64_t)(t4 >> 51);
+    r.l[1] += r.l[0] >> 51;
+    r.l[0] &= MASK51;
+    return r;
+}
+
+inline F sqr(const F& a) { return mul(a, a); }
+
+inline F sqr_n(F x, int n) {
+    for (int i = 0; i < n; i++) x = sqr(x);
+    return x;
+}
+
+// z^(p-2) = z^(2^255 - 21) by the addition chain through z^(2^250 - 1).
+F invert(const F& z) {
+    const F z2 = sqr(z);
+    const F z9 = mul(sqr_n(z2, 2), z);
+    const F z11 = mul(z9, z2);
+    const F e5 = mul(sqr(z11), z9);       // z^(2^5 - 1)
+    const F e10 = mul(sqr_n(e5, 5), e5);  // z^(2^10 - 1)
+    const F e20 = mul(sqr_n(e10, 10), e10);
+    const F e40 = mul(sqr_n(e20, 20), e20);
+    const F e50 = mul(sqr_n(e40, 10), e10);
+    const F e100 = mul(sqr_n(e50, 50), e50);
+    const F e200 = mul(sqr_n(e100, 100), e100);
+    const F e250 = mul(sqr_n(e200, 50), e50);
+    return mul(sqr_n(e250, 5), z11);  // z^(2^255 - 32 + 11)
+}
+
+// Little-endian bytes with bit 255 ignored (RFC 7748 decodeUCoordinate).
+F from_bytes(const uint8_t b[32]) {
+    uint64_t w[4];
+    for (int i = 0; i < 4; i++) {
+        w[i] = 0;
+        for (int j = 7; j >= 0; j--) w[i] = (w[i] << 8) | b[8 * i + j];
+    }
+    w[3] &= 0x7fffffffffffffffull;
+    F r;
+    r.l[0] = w[0] & MASK51;
+    r.l[1] = ((w[0] >> 51) | (w[1] << 13)) & MASK51;
+    r.l[2] = ((w[1] >> 38) | (w[2] << 26)) & MASK51;
+    r.l[3] = ((w[2] >> 25) | (w[3] << 39)) & MASK51;
+    r.l[4] = w[3] >> 12;
+    return r;
+}
+
+// The canonical encoding (the value mod p).
+void to_bytes(uint8_t out[32], F a) {
+    a = carry(carry(a));
+    // Now a < 2^255 + 2^13; a >= p exactly when a + 19 carries out of bit 255.
+    uint64_t q = (a.l[0] + 19) >> 51;
+    for (int i = 1; i < 5; i++) q = (a.l[i] + q) >> 51;
+    a.l[0] += 19 * q;
+    for (int i = 0; i < 4; i++) {
+        a.l[i + 1] += a.l[i] >> 51;
+        a.l[i] &= MASK51;
+    }
+    a.l[4] &= MASK51;
+    const uint64_t w[4] = {a.l[0] | (a.l[1] << 51), (a.l[1] >> 13) | (a.l[2] << 38), (a.l[2] >> 26) | (a.l[3] << 25),
+                           (a.l[3] >> 39) | (a.l[4] << 12)};
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 8; j++) out[8 * i + j] = (uint8_t)(w[i] >> (8 * j));
+}
+
+// u(8B), little-endian.
+const uint8_t U8B_BYTES[32] = {0x68, 0x99, 0xc9, 0x48, 0xed, 0x6f, 0x71, 0xf1, 0x1e, 0xa9, 0x74,
+                               0xad, 0xca, 0xed, 0x78, 0x7a, 0xa1, 0x5c, 0xb6, 0xc8, 0x4d, 0x88,
+                               0x3b, 0xd8, 0x2d, 0x5c, 0xd6, 0xaa, 0xd7, 0xa6, 0x5f, 0x27};
+
+// KeyWalk (main.rs:230-290): u(k + 8n) for n = 0, 1, 2, ...
+struct Walk {
+    F xp, zp, xc, zc, qp, qm;
+    uint64_t next = 0;
+
+    int init(const uint8_t k[32]) {
+        uint8_t prev[32], u[32];
+        lxmfv_previous_scalar(k, prev);
+        if (lxmfv_x25519_base(prev, u) != LXMFV_OK) return LXMFV_ERR_STATE;
+        xp = from_bytes(u);
+        if (lxmfv_x25519_base(k, u) != LXMFV_OK) return LXMFV_ERR_STATE;
+        xc = from_bytes(u);
+        zp = zc = ONE;
+        const F q = from_bytes(U8B_BYTES);
+        qp = add(q, ONE);
+        qm = sub(q, ONE);
+        next = 0;
+        return LXMFV_OK;
+    }
+
+    // The next `len` <= BATCH keys; returns the walk index of the first.
+    uint64_t batch(uint8_t (*out)[32], int len) {
+        F xs[BATCH], zs[BATCH], pre[BATCH];
+        for (int i = 0; i < len; i++) {
+            xs[i] = xc;
+            zs[i] = zc;
+            // P(n+1) = P(n) + Q with P(n) - Q = P(n-1), Q affine.
+            const F t1 = mul(sub(xc, zc), qp), t2 = mul(add(xc, zc), qm);
+            const F xn = mul(zp, sqr(add(t1, t2))), zn = mul(xp, sqr(sub(t1, t2)));
+            xp = xc;
+            zp = zc;
+            xc = xn;
+            zc = zn;
+        }
+        F acc = ONE;
+        for (int i = 0; i < len; i++) {
+            pre[i] = acc;
+            acc = mul(acc, zs[i]);
+        }
+        F inv = invert(acc);
+        for (int i = len - 1; i >= 0; i--) {
+            to_bytes(out[i], mul(xs[i], mul(inv, pre[i])));
+            inv = mul(inv, zs[i]);
+        }
+        const uint64_t first = next;
+        next += (uint64_t)len;
+        return first;
+    }
+};
+
+struct Shared {
+    const uint8_t* prefix;
+    int nibbles;
+    const uint8_t* nh;
+    const int* stop;
+    std::atomic<uint64_t> tries{0};
+    std::atomic<int> found{0}, error{0};
+    uint8_t* identity_out;
+};
+
+inline bool stopped(const Shared& s) {
+    return __atomic_load_n(s.stop, __ATOMIC_RELAXED) != 0 || s.found.load(std::memory_order_relaxed) != 0 ||
+           s.error.load(std::memory_order_relaxed) != 0;
+}
+
+// One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed `ed_seed`.
+template <bool NI>
+void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
+    uint8_t ed_pub[32];
+    Walk w;
+    if (lxmfv_ed25519_public(ed_seed, ed_pub) != LXMFV_OK || w.init(start) != LXMFV_OK) {
+        s->error.store(LXMFV_ERR_STATE);
+        return;
+    }
+    std::vector<uint8_t> keybuf(BATCH * 32);
+    uint8_t(*keys)[32] = reinterpret_cast<uint8_t(*)[32]>(keybuf.data());
+    uint8_t pk[64], block[64], h[16];
+    memcpy(pk + 32, ed_pub, 32);
+    cpu_sha::address_block(s->nh, block);
+    while (!stopped(*s)) {
+        const uint64_t first = w.batch(keys, BATCH);
+        for (int i = 0; i < BATCH; i++) {
+            memcpy(pk, keys[i], 32);
+            cpu_sha::address<NI>(pk, block, h);
+            if (!lxmfv_prefix_matches(s->prefix, s->nibbles, h)) continue;
+            uint8_t ident[64], addr[16];
+            lxmfv_step_scalar(start, first + (uint64_t)i, ident);
+            memcpy(ident + 32, ed_seed, 32);
+            // Recompute from scratch: never hand back a key the fast path got wrong.
+            if (lxmfv_address_of_identity(ident, s->nh, addr) != LXMFV_OK ||
+                !lxmfv_prefix_matches(s->prefix, s->nibbles, addr)) {
+                s->error.store(LXMFV_ERR_RECHECK);
+                return;
+            }
+            int expected = 0;
+            if (s->found.compare_exchange_strong(expected, 1)) memcpy(s->identity_out, ident, 64);
+            s->tries.fetch_add((uint64_t)i + 1, std::memory_order_relaxed);
+            return;
+        }
+        s->tries.fetch_add(BATCH, std::memory_order_relaxed);
+    }
+}
+
+bool use_sha_ni() {
+#if defined(__x86_64__)
+    return cpu_sha::have_sha_ni();
+#else
+    return false;
+#endif
+}
+
+}  // namespace
+
+extern "C" int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out,
+                                   int impl) {
+    if ((count && (!pks || !out)) || !name_hash || impl < 0 || impl > 2) return LXMFV_ERR_ARG;
+    if (impl == 2 && !use_sha_ni()) return LXMFV_ERR_STATE;
+    const bool ni = impl == 2 || (impl == 0 && use_sha_ni());
+    uint8_t block[64];
+    cpu_sha::address_block(name_hash, block);
+    for (uint64_t i = 0; i < count; i++) {
+        if (ni)
+            cpu_sha::address<true>(pks + 64 * i, block, out + 16 * i);
+        else
+            cpu_sha::address<false>(pks + 64 * i, block, out + 16 * i);
+    }
+    return LXMFV_OK;
+}
+
+extern "C" int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys) {
+    if (!start || (count && !keys)) return LXMFV_ERR_ARG;
+    Walk w;
+    if (w.init(start) != LXMFV_OK) return LXMFV_ERR_STATE;
+    std::vector<uint8_t> tmp(BATCH * 32);
+    for (uint64_t done = 0; done < count;) {
+        const int len = (int)std::min<uint64_t>(BATCH, count - done);
+        w.batch(reinterpret_cast<uint8_t(*)[32]>(tmp.data()), len);
+        memcpy(keys + 32 * done, tmp.data(), 32 * (size_t)len);
+        done += (uint64_t)len;
+    }
+    return LXMFV_OK;
+}
+
+extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
+                                const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
+                                uint8_t identity[64]) {
+    if (!prefix || nibbles < 1 || nibbles > 32 || !name_hash || threads < 1 || threads > LXMFV_CPU_MAX_THREADS ||
+        !stop || !identity)
+        return LXMFV_ERR_ARG;
+    if (!seed && first_walker) return LXMFV_ERR_ARG;
+    if (seed && first_walker > (1ull << 24)) return LXMFV_ERR_ARG;
+    // Start scalars and Ed25519 seeds, 32 bytes each per thread.
+    std::vector<uint8_t> starts(32 * (size_t)threads), eds(32 * (size_t)threads);
+    if (seed) {
+        // Walker w of the seeded stream: w = 0 starts at the identity's own
+        // scalar, w >= 1 at the w-th further draw; all share the identity's
+        // Ed25519 seed.  The GPU's seeded lanes use the same numbering.
+        uint8_t ident[64];
+        const uint64_t off = lxmfv_seeded_identity(*seed, ident);
+        const uint64_t last = first_walker + (uint64_t)threads - 1;
+        std::vector<uint8_t> draws(32 * (size_t)std::max<uint64_t>(last, 1));
+        if (last) lxmfv_seeded_scalars(*seed, off, draws.data(), last);
+        for (int t = 0; t < threads; t++) {
+            const uint64_t wk = first_walker + (uint64_t)t;
+            memcpy(&starts[32 * (size_t)t], wk == 0 ? ident : &draws[32 * (wk - 1)], 32);
+            memcpy(&eds[32 * (size_t)t], ident + 32, 32);
+        }
+    } else {
+        // As the reference: each thread its own random scalar and Ed25519 seed.
+        for (int t = 0; t < threads; t++) {
+            uint8_t* k = &starts[32 * (size_t)t];
+            do {
+                if (lxmfv_os_random(k, 32) != LXMFV_OK) return LXMFV_ERR_STATE;
+            } while (!lxmfv_clamp_start(k));
+            if (lxmfv_os_random(&eds[32 * (size_t)t], 32) != LXMFV_OK) return LXMFV_ERR_STATE;
+        }
+    }
+    Shared s;
+    s.prefix = prefix;
+    s.nibbles = nibbles;
+    s.nh = name_hash;
+    s.stop = stop;
+    s.identity_out = identity;
+    std::vector<std::thread> pool;
+    pool.reserve((size_t)threads);
+    const bool ni = use_sha_ni();
+    for (int t = 0; t < threads; t++)
+        pool.emplace_back(ni ? walker<true> : walker<false>, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
+    while (!stopped(s)) {
+        if (tries) __atomic_store_n(tries, s.tries.load(std::memory_order_relaxed), __ATOMIC_RELAXED);
+        std::this_thread::sleep_for(std::chrono::milliseconds(10));
+    }
+    for (auto& th : pool) th.join();
+    if (tries) __atomic_store_n(tries, s.tries.load(), __ATOMIC_RELAXED);
+    if (s.error.load()) return s.error.load();
+    return s.found.load() ? LXMFV_OK : LXMFV_STOPPED;
+}

@@ -126,8 +126,14 @@ SIGNATURES = {
     "lxmfv_pool_keys_per_lane": ([C.c_void_p, C.c_uint32], C.c_uint64),
     "lxmfv_pool_last_step_ms": ([C.c_void_p], C.c_float),
     "lxmfv_pool_close": ([C.c_void_p], None),
+    "lxmfv_cpu_addresses": ([_u8p, C.c_uint64, _u8p, _u8p, C.c_int], C.c_int),
+    "lxmfv_cpu_walk": ([_u8p, C.c_uint64, _u8p], C.c_int),
+    "lxmfv_cpu_search": ([_u8p, C.c_int, _u8p, C.c_int, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_int),
+                          C.POINTER(C.c_uint64), _u8p], C.c_int),
 }
 STATIC_SCRATCH_ELEMS = 131072
+STOPPED = 1
+CPU_MAX_THREADS = 4096
 
 
 def fe_batch_invert_static(d_a: int, d_out: int, count: int, group: int = 64, stream: int | None = None) -> None:
@@ -259,6 +265,60 @@ def address_of_identity(identity: bytes, aspect: str = ASPECT) -> bytes:
     if lib().lxmfv_address_of_identity(_b(identity, 64), _b(name_hash(aspect), 10), out) != OK:
         raise RuntimeError("address recheck failed to run")
     return bytes(out)
+
+
+def cpu_addresses(pks: np.ndarray, aspect: str = ASPECT, impl: int = 0) -> np.ndarray:
+    """lxmf_address on the CPU for (n, 64) public keys; impl 0 auto, 1 portable C, 2 SHA extensions."""
+    pks = np.ascontiguousarray(pks, np.uint8)
+    out = np.zeros((pks.shape[0], 16), np.uint8)
+    rc = lib().lxmfv_cpu_addresses(pks.ctypes.data_as(_u8p), pks.shape[0], _b(name_hash(aspect), 10),
+                                   out.ctypes.data_as(_u8p), impl)
+    if rc != OK:
+        raise LxmfvError(rc, "lxmfv_cpu_addresses failed")
+    return out
+
+
+def cpu_walk(start: bytes, count: int) -> np.ndarray:
+    """KeyWalk on the CPU (main.rs:230-290): the keys u(k + 8n), n < count, as (count, 32) bytes."""
+    out = np.zeros((count, 32), np.uint8)
+    rc = lib().lxmfv_cpu_walk(_b(start, 32), count, out.ctypes.data_as(_u8p))
+    if rc != OK:
+        raise LxmfvError(rc, "lxmfv_cpu_walk failed")
+    return out
+
+
+class CpuSearch:
+    """The CPU search (main.rs:292-323 on `threads` threads, as run_search).
+
+    run() blocks until a hit or stop(); other threads may call stop() and
+    read tries while it runs (the foreign call releases the GIL)."""
+
+    def __init__(self, prefix: tuple[bytes, int], threads: int, aspect: str = ASPECT, seed: int | None = None,
+                 first_walker: int = 0):
+        self.prefix, self.threads, self.aspect = prefix, threads, aspect
+        self.seed, self.first_walker = seed, first_walker
+        self._stop = C.c_int(0)
+        self._tries = C.c_uint64(0)
+
+    def stop(self) -> None:
+        self._stop.value = 1
+
+    @property
+    def tries(self) -> int:
+        return self._tries.value
+
+    def run(self) -> bytes | None:
+        """The rechecked 64-byte identity, or None when stopped first."""
+        ident = (C.c_uint8 * 64)()
+        seed = C.byref(C.c_uint64(self.seed)) if self.seed is not None else None
+        rc = lib().lxmfv_cpu_search(_b(self.prefix[0], 16), self.prefix[1], _b(name_hash(self.aspect), 10),
+                                    self.threads, seed, self.first_walker, C.byref(self._stop),
+                                    C.byref(self._tries), ident)
+        if rc == STOPPED:
+            return None
+        if rc != OK:
+            raise LxmfvError(rc, "lxmfv_cpu_search failed")
+        return bytes(ident)
 
 
 def le_words(b: bytes) -> list[int]:

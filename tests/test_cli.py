@@ -67,6 +67,48 @@ def _check_identity(path, prefix, aspect="lxmf.delivery"):
     return addr.hex()
 
 
+def test_cpu_search_writes_a_valid_identity(tmp_path):
+    r = run(["--threads", "2", "B0C"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Searching on 2 CPU threads; about 4096 tries on average." in r.stdout
+    addr = _check_identity(tmp_path / "b0c.identity", "b0c")
+    assert f"Found {addr}" in r.stdout
+    assert re.search(r"About \d+ tries in [\d.]+ s \(\d+/s\)\. Saved to b0c\.identity", r.stdout)
+
+
+def test_cpu_search_defaults_to_every_core(tmp_path):
+    r = run(["b0"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    m = re.search(r"Searching on (\d+) CPU threads?;", r.stdout)
+    assert m and int(m.group(1)) >= 1
+    assert int(m.group(1)) <= max(cores, os.cpu_count() or 1)
+    _check_identity(tmp_path / "b0.identity", "b0")
+
+
+def test_seeded_cpu_search_finds_the_golden_hit(tmp_path):
+    """One seeded thread walks seed 1's identity scalar: the golden first hit."""
+    import json
+    from oracle import oracle as O
+    with open(os.path.join(ROOT, "tests", "golden", "config1.json")) as f:
+        g = json.load(f)
+    r = run(["--seed", str(g["seed"]), "--threads", "1", g["prefix"]], tmp_path)
+    assert r.returncode == 0, r.stderr
+    want = O.step_scalar(bytes.fromhex(g["scalar"]), g["hits"][0]) + bytes.fromhex(g["ed_seed"])
+    assert (tmp_path / (g["prefix"] + ".identity")).read_bytes() == want
+    assert f"About {g['hits'][0] + 1} tries" in r.stdout
+    _check_identity(tmp_path / (g["prefix"] + ".identity"), g["prefix"])
+
+
+@pytest.mark.gpu
+def test_gpu_and_cpu_together(tmp_path):
+    r = run(["--gpu", "--cpu", "--threads", "2", "B00B"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Searching on 1 GPU and 2 CPU threads" in r.stdout
+    addr = _check_identity(tmp_path / "b00b.identity", "b00b")
+    assert f"Found {addr}" in r.stdout
+
+
 @pytest.mark.gpu
 def test_self_test_passes(tmp_path):
     r = run(["--gpu-self-test"], tmp_path)
