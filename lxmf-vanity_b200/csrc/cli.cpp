@@ -5,6 +5,7 @@
 //   lxmf-vanity --gpu <hex prefix>        search on the GPU(s)
 //   lxmf-vanity --gpu --cpu <hex prefix>  the GPU(s) and the remaining CPU cores together
 //   lxmf-vanity --gpu-self-test           check the GPU against the CPU
+//   lxmf-vanity --gpu --batch-file FILE   many searches at once in the search pool
 //
 // Kept from the reference: the prefix rules (Prefix::parse, main.rs:206-216),
 // refusing to overwrite an identity file (main.rs:467-471), the 64-byte file
@@ -18,7 +19,9 @@
 // Added: --aspect (the destination aspect; default lxmf.delivery), --seed
 // (seeded walkers and identity instead of OS randomness), --devices (one
 // host thread per GPU, first hit wins: fleet.sh's mode in one process),
-// --threads (CPU threads), --walk / --batch / --lanes (kernel choice).
+// --threads (CPU threads), --walk / --batch / --lanes (kernel choice),
+// --batch-file (many searches in one persistent kernel, admitted as lanes free
+// up, each retired on its first hit).
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -52,12 +55,16 @@ const char* USAGE =
     "  --gpu              search on the GPU (NVIDIA B200)\n"
     "  --gpu --cpu        search on the GPU and the remaining CPU cores together\n"
     "  --gpu-self-test    check the GPU's results against the CPU\n"
+    "  --gpu --batch-file FILE\n"
+    "                     run every search of FILE (lines '<hex prefix> [aspect]') together on\n"
+    "                     one GPU; each hit is saved to <prefix>.identity as it comes in\n"
     "options:\n"
     "  --aspect NAME      destination aspect (default lxmf.delivery)\n"
     "  --devices LIST     GPUs to search on, e.g. 0,1,2,3 (default 0); first hit wins\n"
     "  --threads N        CPU threads (default: every core; with --gpu, every core but one)\n"
     "  --seed N           seeded walkers and identity (ChaCha20 stream of N) instead of OS randomness;\n"
-    "                     GPU d uses seed N + d, the CPU threads seed N + (number of GPUs)\n"
+    "                     the d-th GPU listed uses seed N + d, the CPU threads seed N + (number of\n"
+    "                     GPUs); with --batch-file, search i of the file uses seed N + i\n"
     "  --walk group|xadd  the walk (default group; xadd is the x-only differential walk)\n"
     "  --batch N          keys per inversion (default 64)\n"
     "  --lanes N          walker lanes per GPU (default: one full wave)";
@@ -72,7 +79,9 @@ struct Options {
     bool seeded = false;
     uint64_t seed = 0;
     uint32_t walk = LXMFV_WALK_GROUP, batch = 64, lanes = 0;
+    bool batch_given = false;
     int threads = 0;  // CPU threads; 0: the mode's default
+    std::string batch_file;
 };
 
 struct Prefix {
@@ -107,7 +116,8 @@ struct GpuSearch {
 
     ~GpuSearch() { lxmfv_close(h); }
 
-    std::string open(const Options& o, int device) {
+    // `index`: the device's position in --devices, which picks its seed.
+    std::string open(const Options& o, int device, size_t index) {
         lxmfv_options opts{};
         opts.device = device;
         opts.lanes = o.lanes;
@@ -122,8 +132,8 @@ struct GpuSearch {
         desc = buf;
         starts.resize((size_t)lanes * 32);
         if (o.seeded) {
-            // Device d searches with the identity and walkers of seed + d.
-            const uint64_t seed = o.seed + (uint64_t)device;
+            // The d-th device listed searches with the identity and walkers of seed + d.
+            const uint64_t seed = o.seed + (uint64_t)index;
             uint8_t ident[64];
             const uint64_t off = lxmfv_seeded_identity(seed, ident);
             memcpy(starts.data(), ident, 32);
@@ -182,10 +192,10 @@ struct Shared {
 };
 
 // GpuSearch::run (mod.rs:148-174) on one device.
-void run_device(const Options& o, const Prefix& p, int device, Shared& sh) {
+void run_device(const Options& o, const Prefix& p, int device, size_t index, Shared& sh) {
     const auto started = Clock::now();
     GpuSearch g;
-    std::string e = g.open(o, device);
+    std::string e = g.open(o, device, index);
     if (!e.empty()) {
         std::lock_guard<std::mutex> l(sh.mu);
         if (sh.error.empty()) sh.error = "GPU " + std::to_string(device) + " unavailable: " + e;
@@ -266,7 +276,7 @@ void run_cpu(const Options& o, const Prefix& p, int threads, Shared& sh) {
 int self_test(const Options& o) {
     GpuSearch g;
     const auto started = Clock::now();
-    std::string e = g.open(o, o.devices[0]);
+    std::string e = g.open(o, o.devices[0], 0);
     if (!e.empty()) {
         fprintf(stderr, "GPU unavailable: %s\n", e.c_str());
         return 1;
@@ -315,6 +325,252 @@ int self_test(const Options& o) {
     return 0;
 }
 
+// ---- --batch-file: many searches in the search pool. ----
+
+struct BatchSearch {
+    std::string text, aspect, path;
+    Prefix p;
+    uint8_t nh[10], ed_seed[32], ed_pub[32];
+    std::vector<uint8_t> starts;  // 32 bytes per lane
+    uint32_t lanes = 0, id = 0;
+    bool active = false, done = false;
+};
+
+// Lanes for a search of `nibbles` digits: 64 for 5 or fewer, 16 times more per
+// further digit (so expected steps to a hit stay about level), at most 2^17.
+// A function of the search alone, so that its hit does not depend on the mix.
+uint32_t batch_lanes(int nibbles) {
+    double l = 64.0 * std::pow(16.0, std::max(0, nibbles - 5));
+    return (uint32_t)std::min(131072.0, l);
+}
+
+bool read_batch_file(const Options& o, std::vector<BatchSearch>& out) {
+    FILE* f = fopen(o.batch_file.c_str(), "r");
+    if (!f) {
+        fprintf(stderr, "could not read %s: %s\n", o.batch_file.c_str(), strerror(errno));
+        return false;
+    }
+    char line[1024];
+    int lineno = 0;
+    bool ok = true;
+    while (ok && fgets(line, sizeof line, f)) {
+        lineno++;
+        char* hash = strchr(line, '#');
+        if (hash) *hash = 0;
+        char pfx[256] = {0}, asp[512] = {0}, extra[8] = {0};
+        const int n = sscanf(line, "%255s %511s %7s", pfx, asp, extra);
+        if (n <= 0) continue;
+        if (n > 2) {
+            fprintf(stderr, "%s:%d: expected '<hex prefix> [aspect]'\n", o.batch_file.c_str(), lineno);
+            ok = false;
+            break;
+        }
+        BatchSearch b;
+        b.text = pfx;
+        for (auto& c : b.text) c = (char)tolower((unsigned char)c);
+        b.aspect = n == 2 ? asp : o.aspect;
+        b.p.nibbles = lxmfv_prefix_parse(b.text.c_str(), b.p.bytes);
+        if (b.p.nibbles < 0) {
+            fprintf(stderr, "%s:%d: '%s' isn't 1 to 32 hex digits: use 0-9 and a-f only (zero, not the letter O).\n",
+                    o.batch_file.c_str(), lineno, pfx);
+            ok = false;
+            break;
+        }
+        b.path = b.text + ".identity";
+        struct stat st;
+        if (stat(b.path.c_str(), &st) == 0) {
+            fprintf(stderr, "%s already exists; not overwriting it.\n", b.path.c_str());
+            ok = false;
+            break;
+        }
+        for (const auto& prev : out)
+            if (prev.text == b.text) {
+                fprintf(stderr, "%s:%d: prefix %s is listed twice (both would write %s)\n", o.batch_file.c_str(),
+                        lineno, b.text.c_str(), b.path.c_str());
+                ok = false;
+            }
+        out.push_back(std::move(b));
+    }
+    fclose(f);
+    if (ok && out.empty()) {
+        fprintf(stderr, "%s lists no searches\n", o.batch_file.c_str());
+        ok = false;
+    }
+    return ok;
+}
+
+// Start scalars and identity of search i: seeded (seed + i) or from the OS.
+std::string prepare_batch_search(const Options& o, size_t i, BatchSearch& b) {
+    b.lanes = o.lanes ? (o.lanes + 31) / 32 * 32 : batch_lanes(b.p.nibbles);
+    b.starts.resize((size_t)b.lanes * 32);
+    if (o.seeded) {
+        uint8_t ident[64];
+        const uint64_t off = lxmfv_seeded_identity(o.seed + i, ident);
+        memcpy(b.starts.data(), ident, 32);
+        memcpy(b.ed_seed, ident + 32, 32);
+        if (b.lanes > 1) lxmfv_seeded_scalars(o.seed + i, off, b.starts.data() + 32, b.lanes - 1);
+    } else {
+        for (uint32_t t = 0; t < b.lanes; t++) {
+            uint8_t* k = b.starts.data() + 32 * (size_t)t;
+            do {
+                if (lxmfv_os_random(k, 32) != LXMFV_OK) return "no system randomness";
+            } while (!lxmfv_clamp_start(k));
+        }
+        if (lxmfv_os_random(b.ed_seed, 32) != LXMFV_OK) return "no system randomness";
+    }
+    if (lxmfv_ed25519_public(b.ed_seed, b.ed_pub) != LXMFV_OK) return "Ed25519 key derivation failed";
+    lxmfv_name_hash(b.aspect.c_str(), b.nh);
+    return "";
+}
+
+lxmfv_search_desc batch_desc(const BatchSearch& b) {
+    lxmfv_search_desc d{};
+    be_words(b.ed_pub, 8, d.ed);
+    d.name_hash[0] = (uint32_t)b.nh[0] << 24 | (uint32_t)b.nh[1] << 16 | (uint32_t)b.nh[2] << 8 | b.nh[3];
+    d.name_hash[1] = (uint32_t)b.nh[4] << 24 | (uint32_t)b.nh[5] << 16 | (uint32_t)b.nh[6] << 8 | b.nh[7];
+    d.name_hash[2] = (uint32_t)b.nh[8] << 24 | (uint32_t)b.nh[9] << 16;
+    lxmfv_prefix_words(b.p.bytes, b.p.nibbles, d.want, d.mask);
+    d.lanes = b.lanes;
+    return d;
+}
+
+bool write_identity(const std::string& path, const uint8_t ident[64]) {
+    // The file holds a private key: created new, readable only by the owner.
+    const int fd = open(path.c_str(), O_WRONLY | O_CREAT | O_EXCL, 0600);
+    if (fd < 0) {
+        fprintf(stderr, "could not create %s: %s\n", path.c_str(), strerror(errno));
+        return false;
+    }
+    const bool ok = write(fd, ident, 64) == 64;
+    return close(fd) == 0 && ok;
+}
+
+int run_batch_file(const Options& o) {
+    std::vector<BatchSearch> searches;
+    if (!read_batch_file(o, searches)) return 1;
+    const auto start = Clock::now();
+    lxmfv_pool_options po{};
+    po.device = o.devices[0];
+    po.batch = o.batch_given ? o.batch : 0;  // 0: the pool's default group of 256 keys
+    po.max_searches = (uint32_t)std::min<size_t>(4096, searches.size());
+    lxmfv_pool* pool = nullptr;
+    int rc = lxmfv_pool_open(&po, &pool);
+    lxmfv_pool_info_t info{};
+    if (rc == LXMFV_OK) rc = lxmfv_pool_info(pool, &info);
+    if (rc != LXMFV_OK) {
+        fprintf(stderr, "GPU unavailable: %s\n", pool ? lxmfv_pool_last_error(pool) : "out of memory");
+        lxmfv_pool_close(pool);
+        return 2;
+    }
+    for (size_t i = 0; i < searches.size(); i++) {
+        const std::string e = prepare_batch_search(o, i, searches[i]);
+        if (!e.empty()) {
+            fprintf(stderr, "%s\n", e.c_str());
+            lxmfv_pool_close(pool);
+            return 2;
+        }
+        if (searches[i].lanes > info.capacity_lanes) {
+            fprintf(stderr, "%s: %u lanes exceed the pool's %u\n", searches[i].text.c_str(), searches[i].lanes,
+                    info.capacity_lanes);
+            lxmfv_pool_close(pool);
+            return 1;
+        }
+    }
+    printf("%zu searches on the GPU pool (%u lanes, %u keys per group), ready in %.1f s.\n", searches.size(),
+           info.capacity_lanes, info.batch, std::chrono::duration<double>(Clock::now() - start).count());
+    fflush(stdout);
+
+    std::vector<lxmfv_pool_hit> hits(65536);
+    std::vector<int> by_id(po.max_searches, -1);
+    size_t next = 0, found = 0;
+    uint64_t tries = 0;
+    uint32_t groups = 1;
+    int status = 0;
+    auto next_report = Clock::now() + std::chrono::seconds(10);
+    while (found < searches.size() && status == 0) {
+        // Admit waiting searches, in file order, while lanes and slots are free.
+        while (next < searches.size()) {
+            BatchSearch& b = searches[next];
+            const lxmfv_search_desc d = batch_desc(b);
+            rc = lxmfv_pool_submit(pool, &d, b.starts.data(), &b.id);
+            if (rc == LXMFV_ERR_OVERFLOW) break;
+            if (rc != LXMFV_OK) {
+                fprintf(stderr, "GPU: %s\n", lxmfv_pool_last_error(pool));
+                status = 2;
+                break;
+            }
+            b.active = true;
+            by_id[b.id] = (int)next;
+            next++;
+        }
+        if (status) break;
+        uint64_t active_lanes = 0;
+        for (const auto& b : searches) active_lanes += b.active ? b.lanes : 0;
+        uint32_t n = 0;
+        if (lxmfv_pool_step(pool, groups) != LXMFV_OK ||
+            lxmfv_pool_poll(pool, hits.data(), (uint32_t)hits.size(), &n) != LXMFV_OK) {
+            fprintf(stderr, "GPU: %s\n", lxmfv_pool_last_error(pool));
+            status = 2;
+            break;
+        }
+        if (n > hits.size()) {
+            fprintf(stderr, "GPU: %u hits in one step exceed the %zu held; use longer prefixes\n", n, hits.size());
+            status = 2;
+            break;
+        }
+        tries += active_lanes * info.batch * groups;
+        // Per search, the hit with the smallest (n, lane): the first in walk order.
+        std::vector<const lxmfv_pool_hit*> first(po.max_searches, nullptr);
+        for (uint32_t i = 0; i < n; i++) {
+            const lxmfv_pool_hit& h = hits[i];
+            if (h.search >= by_id.size() || by_id[h.search] < 0) continue;
+            const lxmfv_pool_hit*& f = first[h.search];
+            if (!f || h.n < f->n || (h.n == f->n && h.lane < f->lane)) f = &h;
+        }
+        for (uint32_t id = 0; id < first.size() && status == 0; id++) {
+            if (!first[id]) continue;
+            BatchSearch& b = searches[(size_t)by_id[id]];
+            uint8_t ident[64], addr[16];
+            lxmfv_step_scalar(b.starts.data() + 32 * (size_t)first[id]->lane, first[id]->n, ident);
+            memcpy(ident + 32, b.ed_seed, 32);
+            if (lxmfv_address_of_identity(ident, b.nh, addr) != LXMFV_OK ||
+                !lxmfv_prefix_matches(b.p.bytes, b.p.nibbles, addr)) {
+                fprintf(stderr, "GPU hit for %s (lane %u, key %llu) failed its CPU recheck: a kernel bug\n",
+                        b.text.c_str(), first[id]->lane, (unsigned long long)first[id]->n);
+                status = 2;
+                break;
+            }
+            if (!write_identity(b.path, ident)) {
+                status = 1;
+                break;
+            }
+            lxmfv_pool_retire(pool, id);
+            by_id[id] = -1;
+            b.active = false;
+            b.done = true;
+            found++;
+            const uint64_t own = first[id]->n * b.lanes + first[id]->lane + 1;
+            printf("Found %s (%s) after about %llu tries. Saved to %s\n", hex(addr, 16).c_str(), b.aspect.c_str(),
+                   (unsigned long long)own, b.path.c_str());
+            fflush(stdout);
+        }
+        // Grow steps towards about 100 ms of GPU time.
+        if (lxmfv_pool_last_step_ms(pool) < 50.0f && groups < 64) groups *= 2;
+        if (Clock::now() >= next_report) {
+            const double el = std::chrono::duration<double>(Clock::now() - start).count();
+            printf("%zu of %zu found; %.0f tries, %.0f/s\n", found, searches.size(), (double)tries, tries / el);
+            fflush(stdout);
+            next_report += std::chrono::seconds(10);
+        }
+    }
+    lxmfv_pool_close(pool);
+    if (status) return status;
+    const double elapsed = std::chrono::duration<double>(Clock::now() - start).count();
+    printf("All %zu found: about %llu tries in %.1f s (%.0f/s).\n", searches.size(), (unsigned long long)tries,
+           elapsed, (double)tries / elapsed);
+    return 0;
+}
+
 bool parse_devices(const std::string& s, std::vector<int>& out) {
     out.clear();
     size_t i = 0;
@@ -357,8 +613,9 @@ int main(int argc, char** argv) {
         else if (a == "--devices" && value(v) && parse_devices(v, o.devices)) {}
         else if (a == "--seed" && value(v) && parse_u64(v.c_str(), n)) { o.seeded = true; o.seed = n; }
         else if (a == "--walk" && value(v) && (v == "group" || v == "xadd")) o.walk = v == "group" ? LXMFV_WALK_GROUP : LXMFV_WALK_XADD;
-        else if (a == "--batch" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n < 4096) o.batch = (uint32_t)n;
+        else if (a == "--batch" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n < 4096) { o.batch = (uint32_t)n; o.batch_given = true; }
         else if (a == "--lanes" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n < (1ull << 31)) o.lanes = (uint32_t)n;
+        else if (a == "--batch-file" && value(v) && !v.empty()) o.batch_file = v;
         else if (a == "--threads" && value(v) && parse_u64(v.c_str(), n) && n > 0 && n <= LXMFV_CPU_MAX_THREADS) o.threads = (int)n;
         else if (a.rfind("--", 0) == 0) {
             fprintf(stderr, "%s\n", USAGE);
@@ -370,6 +627,13 @@ int main(int argc, char** argv) {
         return 1;
     }
     if (o.self_test) return self_test(o);
+    if (!o.batch_file.empty()) {
+        if (!o.gpu || o.cpu || !words.empty()) {
+            fprintf(stderr, "%s\n", USAGE);
+            return 1;
+        }
+        return run_batch_file(o);
+    }
     if (words.size() != 1) {
         fprintf(stderr, "%s\n", USAGE);
         return 1;
@@ -407,7 +671,8 @@ int main(int argc, char** argv) {
     const auto start = Clock::now();
     std::vector<std::thread> threads;
     if (o.gpu)
-        for (int d : o.devices) threads.emplace_back(run_device, std::cref(o), std::cref(p), d, std::ref(sh));
+        for (size_t i = 0; i < o.devices.size(); i++)
+            threads.emplace_back(run_device, std::cref(o), std::cref(p), o.devices[i], i, std::ref(sh));
     if (cpu_threads) threads.emplace_back(run_cpu, std::cref(o), std::cref(p), cpu_threads, std::ref(sh));
     auto all_tries = [&sh]() { return sh.tries.load() + __atomic_load_n(&sh.cpu_tries, __ATOMIC_RELAXED); };
     auto next_report = start + std::chrono::seconds(10);

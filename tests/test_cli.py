@@ -100,6 +100,73 @@ def test_seeded_cpu_search_finds_the_golden_hit(tmp_path):
     _check_identity(tmp_path / (g["prefix"] + ".identity"), g["prefix"])
 
 
+def test_batch_file_errors(tmp_path):
+    (tmp_path / "ok.txt").write_text("b0\nc1 nomadnetwork.node\n")
+    for args in (["--batch-file", "ok.txt"], ["--gpu", "--cpu", "--batch-file", "ok.txt"],
+                 ["--gpu", "--batch-file", "ok.txt", "b0"]):
+        r = run(args, tmp_path)
+        assert r.returncode == 1 and "usage:" in r.stderr, args
+    cases = {
+        "dup.txt": ("b0\nB0 lxmf.propagation\n", "listed twice"),
+        "extra.txt": ("b0 lxmf.delivery extra\n", "expected '<hex prefix> [aspect]'"),
+        "badhex.txt": ("# a comment\nbo\n", "isn't 1 to 32 hex digits"),
+        "empty.txt": ("\n# nothing\n", "lists no searches"),
+    }
+    for name, (text, msg) in cases.items():
+        (tmp_path / name).write_text(text)
+        r = run(["--gpu", "--batch-file", name], tmp_path)
+        assert r.returncode == 1 and msg in r.stderr, (name, r.stderr)
+    r = run(["--gpu", "--batch-file", "missing.txt"], tmp_path)
+    assert r.returncode == 1 and "could not read" in r.stderr
+    (tmp_path / "c1.identity").write_bytes(b"y" * 64)
+    r = run(["--gpu", "--batch-file", "ok.txt"], tmp_path)
+    assert r.returncode == 1 and "c1.identity already exists" in r.stderr
+    assert (tmp_path / "c1.identity").read_bytes() == b"y" * 64
+
+
+BATCH_LINES = ["b0b", "c0ffe nomadnetwork.node", "d1 lxmf.propagation", "A2C4"]
+
+
+@pytest.mark.gpu
+def test_batch_file_saves_every_identity(tmp_path):
+    (tmp_path / "list.txt").write_text("\n".join(BATCH_LINES) + "\n")
+    r = run(["--gpu", "--batch-file", "list.txt"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "4 searches on the GPU pool" in r.stdout and "All 4 found" in r.stdout
+    for line in BATCH_LINES:
+        prefix, *aspect = line.lower().split()
+        addr = _check_identity(tmp_path / f"{prefix}.identity", prefix, *(aspect or ["lxmf.delivery"]))
+        assert f"Found {addr}" in r.stdout
+
+
+@pytest.mark.gpu
+def test_batch_file_results_are_the_same_alone_and_in_the_mix(tmp_path):
+    """Seeded: search i of the file uses seed N + i, and every lane of the pool
+    advances in step, so each search's identity is the one it finds alone."""
+    mix = tmp_path / "mix"
+    mix.mkdir()
+    (mix / "list.txt").write_text("\n".join(BATCH_LINES) + "\n")
+    r = run(["--gpu", "--seed", "77", "--batch-file", "list.txt"], mix)
+    assert r.returncode == 0, r.stderr
+    for i, line in enumerate(BATCH_LINES):
+        alone = tmp_path / f"alone{i}"
+        alone.mkdir()
+        (alone / "one.txt").write_text(line + "\n")
+        r = run(["--gpu", "--seed", str(77 + i), "--batch-file", "one.txt"], alone)
+        assert r.returncode == 0, r.stderr
+        prefix = line.split()[0].lower()
+        assert (alone / f"{prefix}.identity").read_bytes() == (mix / f"{prefix}.identity").read_bytes(), line
+
+
+@pytest.mark.gpu
+def test_two_replicas_on_one_device(tmp_path):
+    """--devices 0,0: two independent handles (seeds N and N + 1), first hit wins."""
+    r = run(["--gpu", "--devices", "0,0", "--seed", "9", "--lanes", "8192", "b00b"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Searching on 2 GPUs" in r.stdout
+    _check_identity(tmp_path / "b00b.identity", "b00b")
+
+
 @pytest.mark.gpu
 def test_gpu_and_cpu_together(tmp_path):
     r = run(["--gpu", "--cpu", "--threads", "2", "B00B"], tmp_path)
