@@ -35,6 +35,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "lxmf-vanity_b200"))
 
+import lxmfv_replicas as replicas  # noqa: E402  (rank seeds, max over ranks)
+
 TOTAL_KEYS = 1 << 36
 BATCH = 256
 SEED = 3
@@ -359,7 +361,7 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
         wave = b0.threads()
     lanes = a.lanes or wave * max(1, -(-131072 // wave))
     b = lx.Backend(device=dev, lanes=lanes, batch=batch, block=a.block, walk=walk_id, stream=stream.cuda_stream)
-    setup = lx.seeded_setup(SEED + 1000 * rank, lanes)
+    setup = lx.seeded_setup(replicas.rank_seed(SEED, rank), lanes)
     t0 = time.perf_counter()
     b.init_from_scalars(setup.scalars)
     ladder_s = time.perf_counter() - t0
@@ -384,11 +386,8 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
         torch.cuda.synchronize(dev)
     ms = ev0.elapsed_time(ev1)
     hits, n_hits = b.collect()
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = keys_per_step * steps * world / (ms * 1e-3)
+    ms = replicas.max_over_ranks(dist, ms, f"cuda:{dev}")
+    value = replicas.aggregate_rate(keys_per_step * steps, ms * 1e-3, world)
 
     # Every hit is rechecked from scratch on the CPU (OpenSSL), as the reference does.
     pfx = lx.prefix_parse(prefix)
@@ -406,13 +405,9 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
         for _ in range(e2e_steps):
             h, _, _, n = b.launch(args)
             d2h += 4 + 16 * len(h)
-        dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = replicas.max_over_ranks(dist, time.perf_counter() - t0, f"cuda:{dev}")
         import ctypes
-        e2e_line = {"value": keys_per_step * e2e_steps * world / dt, "unit": "keys/s",
+        e2e_line = {"value": replicas.aggregate_rate(keys_per_step * e2e_steps, dt, world), "unit": "keys/s",
                     "h2d_bytes_per_step": ctypes.sizeof(lx.LaunchArgs), "d2h_bytes_per_step": d2h // e2e_steps,
                     "steps": e2e_steps, "api": "lxmfv_launch (C ABI, synchronous, host buffers)"}
 
