@@ -53,6 +53,11 @@ typedef struct lxmfv_handle lxmfv_handle;
  * barrier after every group keeps a block's warps in the same phase of the
  * walk, so they share one phase's code in the instruction cache. */
 #define LXMFV_FLAG_PHASE_SYNC 1u
+/* REGCAP_80 (grouped walk, batch 256, block 256, with PHASE_SYNC): the kernel
+ * built for three blocks per SM, at most 80 registers per thread and 24 warps
+ * per SM, instead of two blocks at up to 128 registers (16 warps).  A point of
+ * the autotuner's register-cap sweep. */
+#define LXMFV_FLAG_REGCAP_80 2u
 
 /* Opening options; zero fields take defaults.
  * Replaces the constants of src/gpu/cuda.rs:13-16 (BATCH, BLOCK,

@@ -32,6 +32,7 @@ struct lxmfv_handle {
     uint32_t batch = 64;  // keys per inversion: B (x-only walk) or G = 2M (grouped walk)
     uint32_t block = 256;
     bool sync = false;    // grouped walk: block barrier after each group
+    bool low_regs = false;  // LXMFV_FLAG_REGCAP_80
     uint32_t* d_state = nullptr;
     uint64_t* d_ns = nullptr;
     uint32_t* d_hit_count = nullptr;
@@ -72,9 +73,16 @@ int fail(lxmfv_handle* h, int code, const char* fmt, ...) {
 constexpr int minb(int block) { return block == 512 ? 1 : block == 256 ? 2 : 4; }
 
 // The kernels for a configuration: block 128 runs without the phase barrier;
-// 256 and 512 with or without it.
+// 256 and 512 with or without it.  `low_regs` (LXMFV_FLAG_REGCAP_80): the
+// G = 256, 256-thread, phase-barrier kernel built for three blocks per SM.
 template <int M>
-const void* group_kernel_ptr(uint32_t block, bool sync) {
+const void* group_kernel_ptr(uint32_t block, bool sync, bool low_regs) {
+    if (low_regs) {
+        if constexpr (M == 128) {
+            if (block == 256 && sync) return (const void*)lxk::group_walk_kernel<128, 256, 3, true>;
+        }
+        return nullptr;
+    }
     if (block == 128) return (const void*)lxk::group_walk_kernel<M, 128, minb(128), false>;
     if (block == 256)
         return sync ? (const void*)lxk::group_walk_kernel<M, 256, minb(256), true>
@@ -86,7 +94,8 @@ const void* group_kernel_ptr(uint32_t block, bool sync) {
 }
 
 template <int B>
-const void* xadd_kernel_ptr(uint32_t block, bool sync) {
+const void* xadd_kernel_ptr(uint32_t block, bool sync, bool low_regs) {
+    if (low_regs) return nullptr;
     if (block == 128) return (const void*)lxk::walk_kernel<B, 128, minb(128), false>;
     if (block == 256)
         return sync ? (const void*)lxk::walk_kernel<B, 256, minb(256), true>
@@ -98,20 +107,20 @@ const void* xadd_kernel_ptr(uint32_t block, bool sync) {
 }
 
 // The walk kernel of a configuration (null when unsupported).
-const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync) {
+const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync, bool low_regs) {
     if (walk == LXMFV_WALK_XADD) {
         switch (batch) {
-            case 16: return xadd_kernel_ptr<16>(block, sync);
-            case 32: return xadd_kernel_ptr<32>(block, sync);
-            case 64: return xadd_kernel_ptr<64>(block, sync);
-            case 128: return xadd_kernel_ptr<128>(block, sync);
+            case 16: return xadd_kernel_ptr<16>(block, sync, low_regs);
+            case 32: return xadd_kernel_ptr<32>(block, sync, low_regs);
+            case 64: return xadd_kernel_ptr<64>(block, sync, low_regs);
+            case 128: return xadd_kernel_ptr<128>(block, sync, low_regs);
         }
     } else if (walk == LXMFV_WALK_GROUP) {
         switch (batch) {
-            case 32: return group_kernel_ptr<16>(block, sync);
-            case 64: return group_kernel_ptr<32>(block, sync);
-            case 128: return group_kernel_ptr<64>(block, sync);
-            case 256: return group_kernel_ptr<128>(block, sync);
+            case 32: return group_kernel_ptr<16>(block, sync, low_regs);
+            case 64: return group_kernel_ptr<32>(block, sync, low_regs);
+            case 128: return group_kernel_ptr<64>(block, sync, low_regs);
+            case 256: return group_kernel_ptr<128>(block, sync, low_regs);
         }
     }
     return nullptr;
@@ -121,7 +130,7 @@ template <int B>
 void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
     typedef void (*fn_t)(lxk::WalkArgs);
-    const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync);
+    const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync, h->low_regs);
     fn<<<grid, h->block, 0, h->stream>>>(wa);
 }
 
@@ -139,7 +148,7 @@ void launch_group(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
     }
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
     typedef void (*fn_t)(lxk::GroupArgs<M>);
-    const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync);
+    const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync, h->low_regs);
     fn<<<grid, h->block, 0, h->stream>>>(ga);
 }
 
@@ -293,9 +302,13 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     // fastest measured on B200 for both walks; otherwise the flags decide.
     h->block = o.block ? o.block : 512;
     h->sync = o.block ? (o.flags & LXMFV_FLAG_PHASE_SYNC) != 0 : true;
+    h->low_regs = (o.flags & LXMFV_FLAG_REGCAP_80) != 0;
     if (h->walk != LXMFV_WALK_GROUP && h->walk != LXMFV_WALK_XADD)
         return fail(h, LXMFV_ERR_ARG, "walk %u: 0 grouped, 1 x-only", h->walk);
-    if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync))
+    if (h->low_regs && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, true))
+        return fail(h, LXMFV_ERR_ARG,
+                    "LXMFV_FLAG_REGCAP_80 needs the grouped walk, batch 256, block 256 and LXMFV_FLAG_PHASE_SYNC");
+    if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
         return fail(h, LXMFV_ERR_ARG,
                     "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
                     "batch 32, 64, 128, 256; block 128, 256 or 512)",
@@ -325,7 +338,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     CU(h, cudaEventCreate(&h->ev0));
     CU(h, cudaEventCreate(&h->ev1));
     int per_sm = 0;
-    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block, h->sync),
+    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs),
                                                         (int)h->block, 0));
     if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
     h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;

@@ -278,6 +278,41 @@ def test_phase_sync_with_a_partial_block(lx, oracle, block):
             assert set(hits) == expected
 
 
+def test_register_capped_kernel_matches_the_oracle(lx, oracle):
+    """LXMFV_FLAG_REGCAP_80 (80 registers, three 256-thread blocks per SM):
+    the same keys, hashes and hits as the oracle, over a partial last block
+    and two launches."""
+    lanes = 1000
+    flags = lx.FLAG_PHASE_SYNC | lx.FLAG_REGCAP_80
+    with lx.Backend(device=0, lanes=lanes, batch=256, block=256, flags=flags) as b:
+        setup = lx.seeded_setup(5150, lanes)
+        b.init_from_scalars(setup.scalars)
+        for launch in range(2):
+            args = lx.make_launch_args(1, setup.ed_pub, lx.prefix_parse("c"), max_hits=1 << 15, dump_threads=lanes,
+                                       dump_keys=256)
+            hits, dump, dump_addr, n = b.launch(args, want_dump=True, want_dump_addr=True)
+            keys = _keys_of(dump, lanes, 256)
+            for t in (0, 255, 256, 767, 999):
+                walked = oracle.walk_keys(bytes(setup.scalars[t]), 512)
+                assert (keys[t] == walked[256 * launch:256 * (launch + 1)]).all(), (t, launch)
+            expected = set()
+            for t in range(lanes):
+                h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, oracle.name_hash(),
+                                            oracle.prefix_parse("c"), 512)
+                expected.update((t, int(x)) for x in h if 256 * launch <= x < 256 * (launch + 1))
+            assert set(hits) == expected and n == len(hits)
+
+
+def test_autotuner_quick_sweep(lx):
+    import lxmfv_tune as tune
+    cfgs = [tune.WalkConfig("group", 256, 512, True), tune.WalkConfig("group", 256, 256, True, regcap=80),
+            tune.WalkConfig("xadd", 128, 512, True)]
+    rows = [tune.measure(c, 0, keys_per_launch=2 ** 28, launches=2) for c in cfgs]
+    assert all(r["keys_per_s"] > 1e9 for r in rows), rows
+    steps = tune.measure_steps(cfgs[0], 0, iters_list=(1, 8), seconds=0.5)
+    assert [s["iters"] for s in steps] == [1, 8] and all(s["keys_per_s"] > 1e9 for s in steps)
+
+
 def test_walks_agree_with_each_other(lx):
     """The grouped and x-only walks give identical hits and dumps for the same lanes."""
     out = []

@@ -136,3 +136,12 @@ def test_launch_args_packing(lx):
     assert list(a.ed)[0] == 0x00010203 and list(a.want) == [0xB00B1000, 0, 0, 0]
     assert list(a.mask) == [0xFFFFF000, 0, 0, 0]
     assert list(a.q) == lx.le_words(lx.U8B)
+
+
+def test_register_cap_needs_its_configuration(lx):
+    """LXMFV_FLAG_REGCAP_80 is checked before any device call (no GPU needed)."""
+    for kw in ({"batch": 128, "block": 256}, {"batch": 256, "block": 512}, {"batch": 256, "block": 256, "walk": 1}):
+        with pytest.raises(lx.LxmfvError, match="REGCAP_80"):
+            lx.Backend(device=0, lanes=256, flags=lx.FLAG_PHASE_SYNC | lx.FLAG_REGCAP_80, **kw)
+    with pytest.raises(lx.LxmfvError, match="REGCAP_80"):
+        lx.Backend(device=0, lanes=256, batch=256, block=256, flags=lx.FLAG_REGCAP_80)
