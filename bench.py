@@ -305,10 +305,10 @@ def main() -> None:
     import torch.distributed as dist
 
     import lxmfv as lx
+    dev = local
+    torch.cuda.set_device(dev)  # before the process group, so each rank's NCCL communicator uses its own GPU
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    dev = local
-    torch.cuda.set_device(dev)
     prefix = _prefix()
     head = measure(torch, dist, lx, a, dev, rank, world, prefix, a.walk, a.batch, a.total_keys, a.steps, a.warmup,
                    e2e=not a.no_e2e)
