@@ -5,7 +5,7 @@ Workload (the plain GPU search): one 8-hex-digit prefix (numpy-seeded),
 aspect lxmf.delivery, every lane starting from its own seeded clamped X25519
 scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, 2^36 keys
 walked in total over the timed steps (a step is one launch that walks every
-lane `iters` groups further).  Keys per inversion: the tuned 256 for the
+lane `iters` groups further).  Keys per inversion: the tuned 512 for the
 headline, and a second measurement at 64 (the reference kernel's BATCH) on a
 quarter of the keys.  Synthetic, seeded inputs; no dataset is involved.
 
@@ -15,7 +15,7 @@ Prints one JSON line on rank 0.  `value` is device-timed (CUDA events on the
 launching stream, max over ranks), `e2e` goes through the C ABI's
 synchronous lxmfv_launch with host buffers, `cpu_baseline` is the restated
 CPU search on this host's cores, `roofline` relates the walk kernel's
-multiply work to the measured IMAD rate of this GPU, and
+ALU-pipe work (ncu counts per key) to the measured ALU rate of this GPU, and
 `reference_cuda_kernel` times the reference's own CUDA kernel on this GPU and
 `cpu_search` this library's CPU search (the reference's default mode).
 With --impl reference, the reference's own kernel body (src/gpu/common.h,
@@ -38,7 +38,7 @@ sys.path.insert(0, os.path.join(ROOT, "lxmf-vanity_b200"))
 import lxmfv_replicas as replicas  # noqa: E402  (rank seeds, max over ranks)
 
 TOTAL_KEYS = 1 << 36
-BATCH = 256
+BATCH = 512
 SEED = 3
 METRIC = "keys/s, plain GPU search (one 8-hex prefix, seeded walkers, 2^36 keys), bit-exact"
 
@@ -53,10 +53,11 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
     return (5 * m + 13) / b, (2 * m + 255) / b
 
 
-# Per key, from one ncu capture of each kernel (profiles/walk_group_g256_plain_search.md,
-# profiles/walk_xadd_b128_plain_search.md): ALU-pipe lane operations (the binding pipe),
-# all instructions, and DRAM bytes (read + write).
+# Per key, from one ncu capture of each kernel (profiles/walk_group_g512_plain_search.md,
+# profiles/walk_group_g256_plain_search.md, profiles/walk_xadd_b128_plain_search.md):
+# ALU-pipe lane operations (the binding pipe), all instructions, and DRAM bytes (read + write).
 NCU_PER_KEY = {
+    ("group", 512): {"alu": 3307, "inst": 5771, "dram_bytes": 30.2},
     ("group", 256): {"alu": 3352, "inst": 5878, "dram_bytes": 28.6},
     ("xadd", 128): {"alu": 4308, "inst": 7909, "dram_bytes": 119.4},
 }
@@ -76,7 +77,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--lanes", type=int, default=0, help="walker lanes per GPU (0: two full waves)")
-    p.add_argument("--batch", type=int, default=BATCH, help="keys per inversion (grouped walk: 32..256)")
+    p.add_argument("--batch", type=int, default=BATCH, help="keys per inversion (grouped walk: 32..512)")
     p.add_argument("--walk", choices=["group", "xadd"], default="group")
     p.add_argument("--block", type=int, default=0)
     p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
@@ -255,12 +256,12 @@ def batched_workload(lx, dev: int, single_value: float) -> dict:
     """256 concurrent searches in the pool's persistent kernel: prefix lengths
     uniform over 4-10 nibbles with random hex, aspects uniform over three, each
     with its own seeded identity; 1184 lanes each, so that the persistent
-    kernel's work items (512 lanes) are exactly 4 per SM; G = 256, 4 groups per
+    kernel's work items (512 lanes) are exactly 4 per SM; G = 512, 4 groups per
     step (the autotuned setting); aggregate device keys/s against the single
     search's `value`."""
     import lxmfv_serve as srv
     specs = srv.batched_specs(256, seed=4, lanes=1184, min_nibbles=4, max_nibbles=10)
-    with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=256) as pool:
+    with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=512) as pool:
         r = srv.run_batched(pool, specs, steps=6, groups=4, warmup=1, recheck_limit=8)
     r["vs_single_search"] = r["keys_per_s"] / single_value
     r["workload"] = "256 searches, 4-10 nibbles, 3 aspects, 1184 lanes each, one persistent launch per step"

@@ -66,7 +66,8 @@ const char* USAGE =
     "                     the d-th GPU listed uses seed N + d, the CPU threads seed N + (number of\n"
     "                     GPUs); with --batch-file, search i of the file uses seed N + i\n"
     "  --walk group|xadd  the walk (default group; xadd is the x-only differential walk)\n"
-    "  --batch N          keys per inversion (default 64)\n"
+    "  --batch N          keys per inversion (default 512; --walk xadd: 128; with --batch-file, keys per\n"
+    "                     group: 256)\n"
     "  --lanes N          walker lanes per GPU (default: one full wave)";
 
 using Clock = std::chrono::steady_clock;
@@ -78,7 +79,7 @@ struct Options {
     std::vector<int> devices{0};
     bool seeded = false;
     uint64_t seed = 0;
-    uint32_t walk = LXMFV_WALK_GROUP, batch = 64, lanes = 0;
+    uint32_t walk = LXMFV_WALK_GROUP, batch = 512, lanes = 0;
     bool batch_given = false;
     int threads = 0;  // CPU threads; 0: the mode's default
     std::string batch_file;
@@ -626,6 +627,8 @@ int main(int argc, char** argv) {
         fprintf(stderr, "%s\n", USAGE);
         return 1;
     }
+    // The fastest keys per inversion of each walk (the x-only walk builds at most 128).
+    if (!o.batch_given && o.walk == LXMFV_WALK_XADD) o.batch = 128;
     if (o.self_test) return self_test(o);
     if (!o.batch_file.empty()) {
         if (!o.gpu || o.cpu || !words.empty()) {

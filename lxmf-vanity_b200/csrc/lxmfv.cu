@@ -121,6 +121,7 @@ const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool 
             case 64: return group_kernel_ptr<32>(block, sync, low_regs);
             case 128: return group_kernel_ptr<64>(block, sync, low_regs);
             case 256: return group_kernel_ptr<128>(block, sync, low_regs);
+            case 512: return group_kernel_ptr<256>(block, sync, low_regs);
         }
     }
     return nullptr;
@@ -173,7 +174,8 @@ void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const
             case 32: launch_group<16>(h, em, iters); break;
             case 64: launch_group<32>(h, em, iters); break;
             case 128: launch_group<64>(h, em, iters); break;
-            default: launch_group<128>(h, em, iters); break;
+            case 256: launch_group<128>(h, em, iters); break;
+            default: launch_group<256>(h, em, iters); break;
         }
     }
 }
@@ -311,7 +313,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
         return fail(h, LXMFV_ERR_ARG,
                     "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
-                    "batch 32, 64, 128, 256; block 128, 256 or 512)",
+                    "batch 32, 64, 128, 256, 512; block 128, 256 or 512)",
                     h->batch, h->block);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);

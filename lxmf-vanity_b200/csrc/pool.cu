@@ -235,6 +235,7 @@ const void* pool_kernel_for(uint32_t batch) {
         case 64: return pool_kernel_ptr<32>();
         case 128: return pool_kernel_ptr<64>();
         case 256: return pool_kernel_ptr<128>();
+        case 512: return pool_kernel_ptr<256>();
     }
     return nullptr;
 }
@@ -266,7 +267,8 @@ void launch_pool_any(lxmfv_pool* p, uint32_t groups) {
     switch (p->batch) {
         case 64: launch_pool<32>(p, groups); break;
         case 128: launch_pool<64>(p, groups); break;
-        default: launch_pool<128>(p, groups); break;
+        case 256: launch_pool<128>(p, groups); break;
+        default: launch_pool<256>(p, groups); break;
     }
 }
 
@@ -323,7 +325,7 @@ int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     p->device = o.device;
     p->batch = o.batch ? o.batch : 256;
     p->m = p->batch / 2;
-    if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128 or 256", p->batch);
+    if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128, 256 or 512", p->batch);
     p->max_searches = o.max_searches ? o.max_searches : 4096;
     p->max_hits = o.max_hits ? o.max_hits : 65536;
     int count = 0;
