@@ -302,15 +302,23 @@ extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uin
         // scalar, w >= 1 at the w-th further draw; all share the identity's
         // Ed25519 seed.  The GPU's seeded lanes use the same numbering.
         uint8_t ident[64];
-        const uint64_t off = lxmfv_seeded_identity(*seed, ident);
+        uint64_t off = lxmfv_seeded_identity(*seed, ident);
+        // Draws 1 .. last come from the stream in order; only this call's
+        // walkers are kept, so memory stays at one chunk whatever first_walker.
         const uint64_t last = first_walker + (uint64_t)threads - 1;
-        std::vector<uint8_t> draws(32 * (size_t)std::max<uint64_t>(last, 1));
-        if (last) lxmfv_seeded_scalars(*seed, off, draws.data(), last);
-        for (int t = 0; t < threads; t++) {
-            const uint64_t wk = first_walker + (uint64_t)t;
-            memcpy(&starts[32 * (size_t)t], wk == 0 ? ident : &draws[32 * (wk - 1)], 32);
-            memcpy(&eds[32 * (size_t)t], ident + 32, 32);
+        constexpr uint64_t CHUNK = 4096;
+        std::vector<uint8_t> chunk(32 * CHUNK);
+        for (uint64_t done = 0; done < last;) {
+            const uint64_t n = std::min(CHUNK, last - done);
+            off = lxmfv_seeded_scalars(*seed, off, chunk.data(), n);
+            for (uint64_t i = 0; i < n; i++) {
+                const uint64_t wk = done + i + 1;
+                if (wk >= first_walker) memcpy(&starts[32 * (size_t)(wk - first_walker)], &chunk[32 * i], 32);
+            }
+            done += n;
         }
+        if (first_walker == 0) memcpy(&starts[0], ident, 32);
+        for (int t = 0; t < threads; t++) memcpy(&eds[32 * (size_t)t], ident + 32, 32);
     } else {
         // As the reference: each thread its own random scalar and Ed25519 seed.
         for (int t = 0; t < threads; t++) {

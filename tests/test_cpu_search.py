@@ -69,7 +69,7 @@ def test_golden_first_hit(lx, config1):
     assert s.tries == n + 1
 
 
-@pytest.mark.parametrize("walker", [0, 3, 1000])
+@pytest.mark.parametrize("walker", [0, 3, 1000, 5000])
 def test_seeded_walker_matches_the_oracle(lx, walker):
     """Thread 0 walks seeded walker `walker`: the first hit of the oracle's
     search over the same walk."""
