@@ -198,19 +198,20 @@ __device__ __forceinline__ void walk_groups(fe& uc, fe& vc, uint64_t& n, uint32_
 }
 
 // The plain search's emission: one prefix for every lane of the launch.
+template <bool DUMP>
 struct LaneEmit {
     const EmitArgs& em;
     uint32_t lane;
     uint64_t key0;
     bool active;
     __device__ __forceinline__ void operator()(const fe& u, uint64_t key) const {
-        if (active) emit_key(em, lane, key, key0, u);
+        if (active) emit_key<DUMP>(em, lane, key, key0, u);
     }
 };
 
 // Threads past the last lane walk a copy of the last lane and neither emit
 // nor store (with SYNC they must still reach every barrier).
-template <int M, int BLOCK, int MINB, bool SYNC>
+template <int M, int BLOCK, int MINB, bool SYNC, bool DUMP>
 static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ GroupArgs<M> a) {
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     if (!SYNC && tid >= a.lanes) return;
@@ -220,7 +221,7 @@ static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __
     fe vc = load_fe(a.state, 1, lane, a.lanes);
     const uint64_t key0 = a.ns[lane];
     uint64_t n = key0;
-    const LaneEmit emit{a.em, lane, key0, active};
+    const LaneEmit<DUMP> emit{a.em, lane, key0, active};
     walk_groups<M, SYNC>(uc, vc, n, a.iters, a.t, emit);
     if (active) {
         store_fe(a.state, 0, lane, a.lanes, uc);

@@ -75,53 +75,65 @@ constexpr int minb(int block) { return block == 512 ? 1 : block == 256 ? 2 : 4; 
 // The kernels for a configuration: block 128 runs without the phase barrier;
 // 256 and 512 with or without it.  `low_regs` (LXMFV_FLAG_REGCAP_80): the
 // G = 256, 256-thread, phase-barrier kernel built for three blocks per SM.
-template <int M>
-const void* group_kernel_ptr(uint32_t block, bool sync, bool low_regs) {
+// DUMP: the build with the dump window's code, for launches that ask for one.
+template <int M, bool DUMP>
+const void* group_kernel_ptr_d(uint32_t block, bool sync, bool low_regs) {
     if (low_regs) {
         if constexpr (M == 128) {
-            if (block == 256 && sync) return (const void*)lxk::group_walk_kernel<128, 256, 3, true>;
+            if (block == 256 && sync) return (const void*)lxk::group_walk_kernel<128, 256, 3, true, DUMP>;
         }
         return nullptr;
     }
-    if (block == 128) return (const void*)lxk::group_walk_kernel<M, 128, minb(128), false>;
+    if (block == 128) return (const void*)lxk::group_walk_kernel<M, 128, minb(128), false, DUMP>;
     if (block == 256)
-        return sync ? (const void*)lxk::group_walk_kernel<M, 256, minb(256), true>
-                    : (const void*)lxk::group_walk_kernel<M, 256, minb(256), false>;
+        return sync ? (const void*)lxk::group_walk_kernel<M, 256, minb(256), true, DUMP>
+                    : (const void*)lxk::group_walk_kernel<M, 256, minb(256), false, DUMP>;
     if (block == 512)
-        return sync ? (const void*)lxk::group_walk_kernel<M, 512, minb(512), true>
-                    : (const void*)lxk::group_walk_kernel<M, 512, minb(512), false>;
+        return sync ? (const void*)lxk::group_walk_kernel<M, 512, minb(512), true, DUMP>
+                    : (const void*)lxk::group_walk_kernel<M, 512, minb(512), false, DUMP>;
+    return nullptr;
+}
+
+template <int M>
+const void* group_kernel_ptr(uint32_t block, bool sync, bool low_regs, bool dump) {
+    return dump ? group_kernel_ptr_d<M, true>(block, sync, low_regs) : group_kernel_ptr_d<M, false>(block, sync, low_regs);
+}
+
+template <int B, bool DUMP>
+const void* xadd_kernel_ptr_d(uint32_t block, bool sync, bool low_regs) {
+    if (low_regs) return nullptr;
+    if (block == 128) return (const void*)lxk::walk_kernel<B, 128, minb(128), false, DUMP>;
+    if (block == 256)
+        return sync ? (const void*)lxk::walk_kernel<B, 256, minb(256), true, DUMP>
+                    : (const void*)lxk::walk_kernel<B, 256, minb(256), false, DUMP>;
+    if (block == 512)
+        return sync ? (const void*)lxk::walk_kernel<B, 512, minb(512), true, DUMP>
+                    : (const void*)lxk::walk_kernel<B, 512, minb(512), false, DUMP>;
     return nullptr;
 }
 
 template <int B>
-const void* xadd_kernel_ptr(uint32_t block, bool sync, bool low_regs) {
-    if (low_regs) return nullptr;
-    if (block == 128) return (const void*)lxk::walk_kernel<B, 128, minb(128), false>;
-    if (block == 256)
-        return sync ? (const void*)lxk::walk_kernel<B, 256, minb(256), true>
-                    : (const void*)lxk::walk_kernel<B, 256, minb(256), false>;
-    if (block == 512)
-        return sync ? (const void*)lxk::walk_kernel<B, 512, minb(512), true>
-                    : (const void*)lxk::walk_kernel<B, 512, minb(512), false>;
-    return nullptr;
+const void* xadd_kernel_ptr(uint32_t block, bool sync, bool low_regs, bool dump) {
+    return dump ? xadd_kernel_ptr_d<B, true>(block, sync, low_regs) : xadd_kernel_ptr_d<B, false>(block, sync, low_regs);
 }
 
 // The walk kernel of a configuration (null when unsupported).
-const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync, bool low_regs) {
+const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync, bool low_regs,
+                            bool dump = false) {
     if (walk == LXMFV_WALK_XADD) {
         switch (batch) {
-            case 16: return xadd_kernel_ptr<16>(block, sync, low_regs);
-            case 32: return xadd_kernel_ptr<32>(block, sync, low_regs);
-            case 64: return xadd_kernel_ptr<64>(block, sync, low_regs);
-            case 128: return xadd_kernel_ptr<128>(block, sync, low_regs);
+            case 16: return xadd_kernel_ptr<16>(block, sync, low_regs, dump);
+            case 32: return xadd_kernel_ptr<32>(block, sync, low_regs, dump);
+            case 64: return xadd_kernel_ptr<64>(block, sync, low_regs, dump);
+            case 128: return xadd_kernel_ptr<128>(block, sync, low_regs, dump);
         }
     } else if (walk == LXMFV_WALK_GROUP) {
         switch (batch) {
-            case 32: return group_kernel_ptr<16>(block, sync, low_regs);
-            case 64: return group_kernel_ptr<32>(block, sync, low_regs);
-            case 128: return group_kernel_ptr<64>(block, sync, low_regs);
-            case 256: return group_kernel_ptr<128>(block, sync, low_regs);
-            case 512: return group_kernel_ptr<256>(block, sync, low_regs);
+            case 32: return group_kernel_ptr<16>(block, sync, low_regs, dump);
+            case 64: return group_kernel_ptr<32>(block, sync, low_regs, dump);
+            case 128: return group_kernel_ptr<64>(block, sync, low_regs, dump);
+            case 256: return group_kernel_ptr<128>(block, sync, low_regs, dump);
+            case 512: return group_kernel_ptr<256>(block, sync, low_regs, dump);
         }
     }
     return nullptr;
@@ -131,7 +143,7 @@ template <int B>
 void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
     typedef void (*fn_t)(lxk::WalkArgs);
-    const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync, h->low_regs);
+    const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync, h->low_regs, wa.em.dump_lanes > 0);
     fn<<<grid, h->block, 0, h->stream>>>(wa);
 }
 
@@ -149,7 +161,7 @@ void launch_group(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
     }
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
     typedef void (*fn_t)(lxk::GroupArgs<M>);
-    const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync, h->low_regs);
+    const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync, h->low_regs, em.dump_lanes > 0);
     fn<<<grid, h->block, 0, h->stream>>>(ga);
 }
 

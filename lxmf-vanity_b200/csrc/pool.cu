@@ -65,6 +65,7 @@ struct PoolArgs {
     uint32_t* hit_count;
     PoolHit* hits;
     uint32_t max_hits;
+    uint32_t one;                  // 1: the SHA-256 sums' multiplier (see madd)
     GroupTable<M> t;
 };
 
@@ -76,9 +77,10 @@ struct PoolEmit {
     uint32_t search;
     uint32_t lane_in_search;
     bool active;
+    uint32_t one;  // from the kernel parameters
     __device__ __forceinline__ void operator()(const fe& u, uint64_t key) const {
         uint32_t d[4];
-        lxsha::dest_hash(u.v, ac.ed, ac, d);
+        lxsha::dest_hash_one(u.v, ac.ed, ac, one, d);
         const bool match = ((d[0] & ac.mask[0]) == ac.want[0]) & ((d[1] & ac.mask[1]) == ac.want[1]) &
                            ((d[2] & ac.mask[2]) == ac.want[2]) & ((d[3] & ac.mask[3]) == ac.want[3]);
         if (active && match) {
@@ -116,7 +118,7 @@ static __global__ void __launch_bounds__(32 * kPoolWarps, 1) pool_walk_kernel(co
         fe uc = load_fe(a.state, 0, lane, a.capacity);
         fe vc = load_fe(a.state, 1, lane, a.capacity);
         uint64_t n = a.ns[lane];
-        const PoolEmit emit{s_ac[warp], a.hit_count, a.hits, a.max_hits, search, a.chunk_first[chunk] + lid, active};
+        const PoolEmit emit{s_ac[warp], a.hit_count, a.hits, a.max_hits, search, a.chunk_first[chunk] + lid, active, a.one};
         walk_groups<M, true>(uc, vc, n, a.groups, a.t, emit);
         if (active) {
             store_fe(a.state, 0, lane, a.capacity, uc);
@@ -256,6 +258,7 @@ void launch_pool(lxmfv_pool* p, uint32_t groups) {
     a.hit_count = p->d_hit_count;
     a.hits = p->d_hits;
     a.max_hits = p->max_hits;
+    a.one = 1;
     for (int i = 0; i <= M; i++) {
         a.t.u[i] = p->tu[i];
         a.t.v[i] = p->tv[i];

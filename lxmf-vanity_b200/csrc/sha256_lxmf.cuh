@@ -170,11 +170,13 @@ __device__ __forceinline__ void iv(uint32_t s[8]) {
 
 // Destination hash (4 big-endian words) of a 64-byte public key whose first
 // 32 bytes are the little-endian words u[0..7] and whose last 32 bytes are
-// the big-endian words hi[0..7].
-__device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi[8], const AddrConsts& c,
-                                          uint32_t out[4]) {
+// the big-endian words hi[0..7].  `one` is the runtime 1 of madd: callers
+// whose search constants live in shared memory pass it from the kernel
+// parameters, so the sums read it from the constant bank (one from shared
+// memory cost the pool kernel 4%).
+__device__ __forceinline__ void dest_hash_one(const uint32_t u[8], const uint32_t hi[8], const AddrConsts& c,
+                                              uint32_t one, uint32_t out[4]) {
     uint32_t w[16], s[8];
-    const uint32_t one = c.one;
     // Block 1: u (byte-swapped to big-endian words) || Ed25519 key.
 #pragma unroll
     for (int i = 0; i < 8; i++) w[i] = __byte_perm(u[i], 0, 0x0123);
@@ -210,6 +212,11 @@ __device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi
     out[1] = s[1] + LXSHA_IV1;
     out[2] = s[2] + LXSHA_IV2;
     out[3] = s[3] + LXSHA_IV3;
+}
+
+__device__ __forceinline__ void dest_hash(const uint32_t u[8], const uint32_t hi[8], const AddrConsts& c,
+                                          uint32_t out[4]) {
+    dest_hash_one(u, hi, c, c.one, out);
 }
 
 }  // namespace lxsha

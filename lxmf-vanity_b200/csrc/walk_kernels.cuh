@@ -72,7 +72,10 @@ __device__ __forceinline__ void store_fe(uint32_t* st, int e, uint32_t lane, uin
 }
 
 // u(key) is final and canonical: hash, compare, record.  key0 is the lane's
-// first walk index in this launch (the dump window starts there).
+// first walk index in this launch (the dump window starts there).  DUMP: the
+// kernel was launched with a dump window; launches without one run kernels
+// built without the dump code (the per-key test and stores cost 0.7%).
+template <bool DUMP>
 __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint64_t key, uint64_t key0, const fe& u) {
     uint32_t d[4];
     lxsha::dest_hash(u.v, a.ac.ed, a.ac, d);
@@ -86,7 +89,7 @@ __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint6
             a.hits[slot].n = key;
         }
     }
-    if (lane < a.dump_lanes) {
+    if (DUMP && lane < a.dump_lanes) {
         const uint64_t m = key - key0;
         if (m < a.dump_keys) {
             const size_t at = (size_t)lane * a.dump_keys + m;
@@ -105,7 +108,7 @@ __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint6
 // SYNC: a block barrier after each batch keeps the block's warps in the same
 // phase (see group_walk_kernel); threads past the last lane then walk a copy
 // of the last lane and neither emit nor store.
-template <int B, int BLOCK, int MINB, bool SYNC>
+template <int B, int BLOCK, int MINB, bool SYNC, bool DUMP>
 static __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_constant__ WalkArgs a) {
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     if (!SYNC && tid >= a.lanes) return;
@@ -141,7 +144,7 @@ static __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_c
         for (int i = B - 1; i >= 0; --i) {
             const fe u = fe_canon(fe_mul(ys[i], inv));
             inv = fe_mul(inv, zs[i]);
-            if (active) emit_key(a.em, lane, n + (uint64_t)i, key0, u);
+            if (active) emit_key<DUMP>(a.em, lane, n + (uint64_t)i, key0, u);
         }
         n += B;
         if (SYNC) __syncthreads();
