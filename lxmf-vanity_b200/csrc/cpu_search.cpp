@@ -4,11 +4,12 @@
 // search; the GPU entry points never fall back to it.
 //
 // Per thread, as the reference: one start scalar k and one Ed25519 seed; the
-// X25519 keys u(k + 8n) by x-only differential addition of Q = 8B, 256 at a
-// time with their Z coordinates inverted together (Montgomery's trick); each
+// X25519 keys u(k + 8n), 256 at a time, in walk order (the reference's
+// KeyWalk uses x-only differential addition; here the grouped affine walk of
+// the GPU kernels visits the same keys with a third of the field work); each
 // key's address by the double SHA-256 (cpu_sha256.h: the x86 SHA extensions
-// where present); a hit is rebuilt from its scalar and rechecked from scratch
-// (OpenSSL) before it is returned.
+// where present); the first match in walk order is rebuilt from its scalar and
+// rechecked from scratch (OpenSSL) before it is returned.
 // Field: GF(2^255-19) in 5 x 51-bit limbs with 128-bit products.
 #include <algorithm>
 #include <atomic>
@@ -24,7 +25,7 @@ namespace {
 
 typedef unsigned __int128 u128;
 constexpr uint64_t MASK51 = (1ull << 51) - 1;
-constexpr int BATCH = 256;  // keys per inversion, as main.rs's BATCH
+constexpr int BATCH = 256;  // keys per batch inversion (a group), as main.rs's BATCH
 
 struct F {
     uint64_t l[5];
@@ -144,52 +145,144 @@ const uint8_t U8B_BYTES[32] = {0x68, 0x99, 0xc9, 0x48, 0xed, 0x6f, 0x71, 0xf1, 0
                                0xad, 0xca, 0xed, 0x78, 0x7a, 0xa1, 0x5c, 0xb6, 0xc8, 0x4d, 0x88,
                                0x3b, 0xd8, 0x2d, 0x5c, 0xd6, 0xaa, 0xd7, 0xa6, 0x5f, 0x27};
 
-// KeyWalk (main.rs:230-290): u(k + 8n) for n = 0, 1, 2, ...
+// v(8B), the even square root of u^3 + A u^2 + u at u = u(8B), little-endian 32-bit words.
+const uint32_t V8B_WORDS[8] = {0x9f728718u, 0xc5296d6eu, 0x70c591f9u, 0x4f479c67u,
+                               0x4066b08cu, 0x8dcf4469u, 0x8fb939e4u, 0x6085bbbau};
+
+constexpr int HALF = BATCH / 2;  // M: a group is the 2M = BATCH keys around one centre
+
+F from_words(const uint32_t w[8]) {
+    uint8_t b[32];
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 4; j++) b[4 * i + j] = (uint8_t)(w[i] >> (8 * j));
+    return from_bytes(b);
+}
+
+F small(uint64_t x) { return F{{x, 0, 0, 0, 0}}; }
+
+// P1 + P2 on the Montgomery curve v^2 = u^3 + A u^2 + u (affine, P1 != +-P2).
+void add_affine(const F& u1, const F& v1, const F& u2, const F& v2, F& u3, F& v3) {
+    const F l = mul(sub(v2, v1), invert(sub(u2, u1)));
+    u3 = sub(sub(sub(sqr(l), small(486662)), u1), u2);
+    v3 = sub(mul(l, sub(u1, u3)), v1);
+}
+
+// The group table: T_i = i Q (i = 1..M) and T_0 = J = 2M Q, affine, with
+// Q = 8B = (u(8B), v(8B)); built once by affine additions.
+struct GroupTable {
+    F u[HALF + 1], v[HALF + 1];
+    GroupTable() {
+        const F uq = from_bytes(U8B_BYTES), vq = from_words(V8B_WORDS);
+        // T_2 = 2Q by the tangent: l = (3u^2 + 2Au + 1) / 2v.
+        const F l = mul(add(add(mul(small(3), sqr(uq)), mul(small(2 * 486662), uq)), ONE), invert(add(vq, vq)));
+        F tu = sub(sub(sqr(l), small(486662)), add(uq, uq));
+        F tv = sub(mul(l, sub(uq, tu)), vq);
+        u[1] = uq;
+        v[1] = vq;
+        u[2] = tu;
+        v[2] = tv;
+        for (int i = 3; i <= 2 * HALF; i++) {
+            F nu, nv;
+            add_affine(tu, tv, uq, vq, nu, nv);
+            tu = nu;
+            tv = nv;
+            if (i <= HALF) {
+                u[i] = tu;
+                v[i] = tv;
+            }
+        }
+        u[0] = tu;
+        v[0] = tv;
+    }
+};
+
+const GroupTable& group_table() {
+    static const GroupTable t;  // thread-safe initialisation (C++11)
+    return t;
+}
+
+// u(k + 8n) for n = 0, 1, 2, ... by the grouped affine walk, the same keys as
+// KeyWalk (main.rs:230-290) with about a third of its field work: keys
+// C - i Q and C + i Q share the denominator u_{iQ} - u_C, so one batch
+// inversion over M + 1 denominators serves a whole group of 2M keys and the
+// step to the next centre C + 2M Q.  Each group's keys come out in walk order.
 struct Walk {
-    F xp, zp, xc, zc, qp, qm;
+    F uc, vc;
     uint64_t next = 0;
+    uint8_t buf[BATCH][32];
 
     int init(const uint8_t k[32]) {
-        uint8_t prev[32], u[32];
+        // y of P = kB = (k/8) Q from u(k - 8) and u(k) (Okeya-Sakurai recovery
+        // with -Q, since P - Q is the known neighbour), then C = P + M Q.
+        uint8_t prev[32], b[32];
         lxmfv_previous_scalar(k, prev);
-        if (lxmfv_x25519_base(prev, u) != LXMFV_OK) return LXMFV_ERR_STATE;
-        xp = from_bytes(u);
-        if (lxmfv_x25519_base(k, u) != LXMFV_OK) return LXMFV_ERR_STATE;
-        xc = from_bytes(u);
-        zp = zc = ONE;
-        const F q = from_bytes(U8B_BYTES);
-        qp = add(q, ONE);
-        qm = sub(q, ONE);
+        if (lxmfv_x25519_base(prev, b) != LXMFV_OK) return LXMFV_ERR_STATE;
+        const F um8 = from_bytes(b);
+        if (lxmfv_x25519_base(k, b) != LXMFV_OK) return LXMFV_ERR_STATE;
+        const F uk = from_bytes(b);
+        const F xp = from_bytes(U8B_BYTES), yp = sub(F{{0, 0, 0, 0, 0}}, from_words(V8B_WORDS));
+        // recover_y with (X1:Z1) = (uk:1), (X2:Z2) = (um8:1)
+        F v1 = xp;
+        F v2 = add(uk, v1);
+        F v3 = sub(uk, v1);
+        v3 = mul(sqr(v3), um8);
+        v1 = small(2 * 486662);
+        v2 = add(v2, v1);
+        const F v4 = add(mul(xp, uk), ONE);
+        v2 = mul(v2, v4);
+        v2 = sub(v2, v1);
+        const F Y = sub(v2, v3);
+        const F c = add(yp, yp);
+        const F zi = invert(c);
+        const F pu = uk, pv = mul(Y, zi);  // X = c uk, Z = c: u = uk
+        const GroupTable& t = group_table();
+        add_affine(pu, pv, t.u[HALF], t.v[HALF], uc, vc);
         next = 0;
         return LXMFV_OK;
     }
 
-    // The next `len` <= BATCH keys; returns the walk index of the first.
-    uint64_t batch(uint8_t (*out)[32], int len) {
-        F xs[BATCH], zs[BATCH], pre[BATCH];
-        for (int i = 0; i < len; i++) {
-            xs[i] = xc;
-            zs[i] = zc;
-            // P(n+1) = P(n) + Q with P(n) - Q = P(n-1), Q affine.
-            const F t1 = mul(sub(xc, zc), qp), t2 = mul(add(xc, zc), qm);
-            const F xn = mul(zp, sqr(add(t1, t2))), zn = mul(xp, sqr(sub(t1, t2)));
-            xp = xc;
-            zp = zc;
-            xc = xn;
-            zc = zn;
-        }
-        F acc = ONE;
-        for (int i = 0; i < len; i++) {
+    // The group of keys next .. next + BATCH - 1 into buf, in walk order.
+    void group() {
+        const GroupTable& t = group_table();
+        F pre[HALF + 1];
+        F acc = sub(t.u[0], uc);
+        for (int i = 1; i <= HALF; i++) {
             pre[i] = acc;
-            acc = mul(acc, zs[i]);
+            acc = mul(acc, sub(t.u[i], uc));
         }
         F inv = invert(acc);
-        for (int i = len - 1; i >= 0; i--) {
-            to_bytes(out[i], mul(xs[i], mul(inv, pre[i])));
-            inv = mul(inv, zs[i]);
+        const F s0 = add(uc, small(486662));
+        F vnext = vc, unext = uc;
+        for (int i = HALF; i >= 0; i--) {
+            F invi = inv;  // 1 / (u_{T_i} - u_C)
+            if (i > 0) {
+                invi = mul(inv, pre[i]);
+                inv = mul(inv, sub(t.u[i], uc));
+            }
+            const F sum = add(s0, t.u[i]);
+            const F lp = mul(sub(t.v[i], vc), invi);
+            const F up = sub(sqr(lp), sum);  // C + T_i (i = 0: the next centre C + J)
+            if (i > 0) {
+                const F lm = mul(add(t.v[i], vc), invi);
+                to_bytes(buf[HALF - i], sub(sqr(lm), sum));  // C - T_i: key c - i
+                if (i < HALF) to_bytes(buf[HALF + i], up);    // C + T_i: key c + i
+            } else {
+                to_bytes(buf[HALF], uc);  // the centre: key c
+                vnext = sub(mul(lp, sub(uc, up)), vc);
+                unext = up;
+            }
         }
+        uc = unext;
+        vc = vnext;
+    }
+
+    // The next `len` <= BATCH keys (a whole group; a shorter request keeps its
+    // first keys and ends the walk); returns the walk index of the first.
+    uint64_t batch(uint8_t (*out)[32], int len) {
+        group();
+        memcpy(out, buf, 32 * (size_t)len);
         const uint64_t first = next;
-        next += (uint64_t)len;
+        next += BATCH;
         return first;
     }
 };
