@@ -302,6 +302,19 @@ inline bool stopped(const Shared& s) {
            s.error.load(std::memory_order_relaxed) != 0;
 }
 
+// The addresses of two public keys.
+template <bool NI>
+inline void hash_pair(uint8_t pk[2][64], uint8_t blocks[2][64], uint8_t h[2][16]) {
+#if defined(__x86_64__)
+    if (NI) {
+        cpu_sha::address2_ni(pk[0], pk[1], blocks, h[0], h[1]);
+        return;
+    }
+#endif
+    cpu_sha::address<false>(pk[0], blocks[0], h[0]);
+    cpu_sha::address<false>(pk[1], blocks[1], h[1]);
+}
+
 // One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed `ed_seed`.
 template <bool NI>
 void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
@@ -313,15 +326,22 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     }
     std::vector<uint8_t> keybuf(BATCH * 32);
     uint8_t(*keys)[32] = reinterpret_cast<uint8_t(*)[32]>(keybuf.data());
-    uint8_t pk[64], block[64], h[16];
-    memcpy(pk + 32, ed_pub, 32);
-    cpu_sha::address_block(s->nh, block);
+    uint8_t pk[2][64], blocks[2][64], h[2][16];
+    for (int j = 0; j < 2; j++) {
+        memcpy(pk[j] + 32, ed_pub, 32);
+        cpu_sha::address_block(s->nh, blocks[j]);
+    }
     while (!stopped(*s)) {
         const uint64_t first = w.batch(keys, BATCH);
         for (int i = 0; i < BATCH; i++) {
-            memcpy(pk, keys[i], 32);
-            cpu_sha::address<NI>(pk, block, h);
-            if (!lxmfv_prefix_matches(s->prefix, s->nibbles, h)) continue;
+            // Keys are hashed in pairs (two SHA-256 streams interleaved where the
+            // CPU has the SHA extensions) and checked in walk order.
+            if ((i & 1) == 0) {
+                memcpy(pk[0], keys[i], 32);
+                memcpy(pk[1], keys[i + 1], 32);
+                hash_pair<NI>(pk, blocks, h);
+            }
+            if (!lxmfv_prefix_matches(s->prefix, s->nibbles, h[i & 1])) continue;
             uint8_t ident[64], addr[16];
             lxmfv_step_scalar(start, first + (uint64_t)i, ident);
             memcpy(ident + 32, ed_seed, 32);
@@ -352,8 +372,20 @@ bool use_sha_ni() {
 
 extern "C" int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out,
                                    int impl) {
-    if ((count && (!pks || !out)) || !name_hash || impl < 0 || impl > 2) return LXMFV_ERR_ARG;
-    if (impl == 2 && !use_sha_ni()) return LXMFV_ERR_STATE;
+    if ((count && (!pks || !out)) || !name_hash || impl < 0 || impl > 3) return LXMFV_ERR_ARG;
+    if (impl >= 2 && !use_sha_ni()) return LXMFV_ERR_STATE;
+#if defined(__x86_64__)
+    if (impl == 3) {
+        uint8_t blocks[2][64];
+        cpu_sha::address_block(name_hash, blocks[0]);
+        cpu_sha::address_block(name_hash, blocks[1]);
+        uint64_t i = 0;
+        for (; i + 1 < count; i += 2)
+            cpu_sha::address2_ni(pks + 64 * i, pks + 64 * (i + 1), blocks, out + 16 * i, out + 16 * (i + 1));
+        if (i < count) cpu_sha::address<true>(pks + 64 * i, blocks[0], out + 16 * i);
+        return LXMFV_OK;
+    }
+#endif
     const bool ni = impl == 2 || (impl == 0 && use_sha_ni());
     uint8_t block[64];
     cpu_sha::address_block(name_hash, block);

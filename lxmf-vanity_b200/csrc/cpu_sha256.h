@@ -96,6 +96,53 @@ __attribute__((target("sha,sse4.1"))) inline void compress_ni(uint32_t s[8], con
     _mm_storeu_si128((__m128i*)&s[4], _mm_alignr_epi8(cdgh, t, 8));      // e f g h
 }
 
+// Two compressions at once: two independent blocks into two states, their
+// instructions interleaved so that one stream's sha256rnds2 latency hides
+// behind the other's.  The schedule is kept as a rolling window of four
+// message vectors per stream (twelve XMM registers in all).
+__attribute__((target("sha,sse4.1"))) inline void compress_ni2(uint32_t s0[8], const uint8_t* p0, uint32_t s1[8],
+                                                              const uint8_t* p1) {
+    const __m128i bswap = _mm_set_epi64x(0x0c0d0e0f08090a0bll, 0x0405060700010203ll);
+    uint32_t* st[2] = {s0, s1};
+    const uint8_t* pp[2] = {p0, p1};
+    __m128i abef[2], cdgh[2], abef0[2], cdgh0[2], m[2][4];
+    for (int j = 0; j < 2; j++) {
+        __m128i t = _mm_shuffle_epi32(_mm_loadu_si128((const __m128i*)&st[j][0]), 0xB1);
+        __m128i c = _mm_shuffle_epi32(_mm_loadu_si128((const __m128i*)&st[j][4]), 0x1B);
+        abef[j] = _mm_alignr_epi8(t, c, 8);
+        cdgh[j] = _mm_blend_epi16(c, t, 0xF0);
+        abef0[j] = abef[j];
+        cdgh0[j] = cdgh[j];
+        for (int i = 0; i < 4; i++) m[j][i] = _mm_shuffle_epi8(_mm_loadu_si128((const __m128i*)(pp[j] + 16 * i)), bswap);
+    }
+    for (int i = 0; i < 16; i++) {
+        const __m128i k = _mm_loadu_si128((const __m128i*)&K[4 * i]);
+        for (int j = 0; j < 2; j++) {
+            __m128i w;
+            if (i < 4) {
+                w = m[j][i];
+            } else {
+                // W[4i..4i+3] from the last four vectors (slot i & 3 holds W[4(i-4)..]).
+                const __m128i x = _mm_add_epi32(_mm_sha256msg1_epu32(m[j][i & 3], m[j][(i + 1) & 3]),
+                                                _mm_alignr_epi8(m[j][(i + 3) & 3], m[j][(i + 2) & 3], 4));
+                w = _mm_sha256msg2_epu32(x, m[j][(i + 3) & 3]);
+                m[j][i & 3] = w;
+            }
+            __m128i wk = _mm_add_epi32(w, k);
+            cdgh[j] = _mm_sha256rnds2_epu32(cdgh[j], abef[j], wk);
+            wk = _mm_shuffle_epi32(wk, 0x0E);
+            abef[j] = _mm_sha256rnds2_epu32(abef[j], cdgh[j], wk);
+        }
+    }
+    for (int j = 0; j < 2; j++) {
+        const __m128i a = _mm_add_epi32(abef[j], abef0[j]), c = _mm_add_epi32(cdgh[j], cdgh0[j]);
+        const __m128i t = _mm_shuffle_epi32(a, 0x1B);
+        const __m128i u = _mm_shuffle_epi32(c, 0xB1);
+        _mm_storeu_si128((__m128i*)&st[j][0], _mm_blend_epi16(t, u, 0xF0));
+        _mm_storeu_si128((__m128i*)&st[j][4], _mm_alignr_epi8(u, t, 8));
+    }
+}
+
 inline bool have_sha_ni() {
     static const bool yes = __builtin_cpu_supports("sha") && __builtin_cpu_supports("sse4.1");
     return yes;
@@ -147,6 +194,38 @@ inline void address(const uint8_t pk[64], uint8_t block[64], uint8_t out[16]) {
         out[4 * i + 3] = (uint8_t)s[i];
     }
 }
+
+#if defined(__x86_64__)
+// address() for two public keys at once with the SHA extensions.  `blocks`
+// is two 64-byte buffers, each set up by address_block.
+inline void address2_ni(const uint8_t pk0[64], const uint8_t pk1[64], uint8_t blocks[2][64], uint8_t out0[16],
+                        uint8_t out1[16]) {
+    uint32_t s0[8], s1[8];
+    memcpy(s0, IV, sizeof s0);
+    memcpy(s1, IV, sizeof s1);
+    compress_ni2(s0, pk0, s1, pk1);
+    compress_ni2(s0, pad64(), s1, pad64());
+    uint32_t* st[2] = {s0, s1};
+    for (int j = 0; j < 2; j++)
+        for (int i = 0; i < 4; i++) {
+            blocks[j][10 + 4 * i] = (uint8_t)(st[j][i] >> 24);
+            blocks[j][11 + 4 * i] = (uint8_t)(st[j][i] >> 16);
+            blocks[j][12 + 4 * i] = (uint8_t)(st[j][i] >> 8);
+            blocks[j][13 + 4 * i] = (uint8_t)st[j][i];
+        }
+    memcpy(s0, IV, sizeof s0);
+    memcpy(s1, IV, sizeof s1);
+    compress_ni2(s0, blocks[0], s1, blocks[1]);
+    uint8_t* out[2] = {out0, out1};
+    for (int j = 0; j < 2; j++)
+        for (int i = 0; i < 4; i++) {
+            out[j][4 * i] = (uint8_t)(st[j][i] >> 24);
+            out[j][4 * i + 1] = (uint8_t)(st[j][i] >> 16);
+            out[j][4 * i + 2] = (uint8_t)(st[j][i] >> 8);
+            out[j][4 * i + 3] = (uint8_t)st[j][i];
+        }
+}
+#endif
 
 // Sets up the second hash's block: name hash and padding.
 inline void address_block(const uint8_t nh[10], uint8_t block[64]) {
