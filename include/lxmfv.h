@@ -65,7 +65,7 @@ typedef struct lxmfv_handle lxmfv_handle;
 typedef struct {
     int32_t device;       /* CUDA device ordinal */
     uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
-    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 512; 0: 64 */
+    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 512; 0: the fastest (GROUP 512, XADD 128) */
     uint32_t block;       /* threads per block: 128, 256 (512: grouped walk only); 0: 256 */
     uint32_t walk;        /* LXMFV_WALK_GROUP (0, default) or LXMFV_WALK_XADD */
     uint32_t flags;       /* LXMFV_FLAG_* */

@@ -311,7 +311,8 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     if (opts) o = *opts;
     h->device = o.device;
     h->walk = o.walk;
-    h->batch = o.batch ? o.batch : 64;
+    // 0: the fastest keys per inversion of each walk (the autotuner's choice).
+    h->batch = o.batch ? o.batch : (o.walk == LXMFV_WALK_XADD ? 128 : 512);
     // Default launch shape (block 0): 512 threads with the phase barrier, the
     // fastest measured on B200 for both walks; otherwise the flags decide.
     h->block = o.block ? o.block : 512;

@@ -341,9 +341,10 @@ def test_bad_step_point_rejected(backend, lx):
 
 def test_self_test_shape(lx):
     """The reference's --gpu-self-test (mod.rs:178-207) on the default-sized
-    device: the first batch of 256 lanes against plain X25519, >= 100 hits for
-    'b0' with iters = 1, every hit rechecked from scratch on the CPU."""
-    with lx.Backend(device=0) as b:
+    device: the first batch (64 keys, the reference's BATCH) of 256 lanes against
+    plain X25519, >= 100 hits for 'b0' with iters = 1, every hit rechecked from
+    scratch on the CPU."""
+    with lx.Backend(device=0, batch=64) as b:
         lanes = b.threads()
         assert lanes >= 256
         starts = np.stack([np.frombuffer(lx.random_start_scalar(), np.uint8) for _ in range(256)])
