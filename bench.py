@@ -57,7 +57,7 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
 # profiles/walk_group_g256_plain_search.md, profiles/walk_xadd_b128_plain_search.md):
 # ALU-pipe lane operations (the binding pipe), all instructions, and DRAM bytes (read + write).
 NCU_PER_KEY = {
-    ("group", 512): {"alu": 3313, "inst": 5761, "dram_bytes": 30.4},
+    ("group", 512): {"alu": 3298, "inst": 5826, "dram_bytes": 31.6},
     ("group", 256): {"alu": 3352, "inst": 5878, "dram_bytes": 28.6},
     ("xadd", 128): {"alu": 4308, "inst": 7909, "dram_bytes": 119.4},
 }
