@@ -67,7 +67,7 @@ const char* USAGE =
     "                     GPUs); with --batch-file, search i of the file uses seed N + i\n"
     "  --walk group|xadd  the walk (default group; xadd is the x-only differential walk)\n"
     "  --batch N          keys per inversion (default 512; --walk xadd: 128; with --batch-file, keys per\n"
-    "                     group: 256)\n"
+    "                     group: 512)\n"
     "  --lanes N          walker lanes per GPU (default: one full wave)";
 
 using Clock = std::chrono::steady_clock;
@@ -452,7 +452,7 @@ int run_batch_file(const Options& o) {
     const auto start = Clock::now();
     lxmfv_pool_options po{};
     po.device = o.devices[0];
-    po.batch = o.batch_given ? o.batch : 0;  // 0: the pool's default group of 256 keys
+    po.batch = o.batch_given ? o.batch : 0;  // 0: the pool's default group of 512 keys
     po.max_searches = (uint32_t)std::min<size_t>(4096, searches.size());
     lxmfv_pool* pool = nullptr;
     int rc = lxmfv_pool_open(&po, &pool);

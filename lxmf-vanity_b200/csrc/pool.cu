@@ -326,7 +326,7 @@ int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     lxmfv_pool_options o{};
     if (opts) o = *opts;
     p->device = o.device;
-    p->batch = o.batch ? o.batch : 256;
+    p->batch = o.batch ? o.batch : 512;  // 0: the autotuner's choice on the batched mix
     p->m = p->batch / 2;
     if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128, 256 or 512", p->batch);
     p->max_searches = o.max_searches ? o.max_searches : 4096;
