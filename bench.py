@@ -59,7 +59,7 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
 NCU_PER_KEY = {
     ("group", 512): {"alu": 3298, "inst": 5826, "dram_bytes": 31.6},
     ("group", 256): {"alu": 3352, "inst": 5878, "dram_bytes": 28.6},
-    ("xadd", 128): {"alu": 4308, "inst": 7909, "dram_bytes": 119.4},
+    ("xadd", 128): {"alu": 4282, "inst": 8093, "dram_bytes": 131.9},
 }
 
 
