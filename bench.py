@@ -58,7 +58,7 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
 # ALU-pipe lane operations (the binding pipe), all instructions, and DRAM bytes (read + write).
 NCU_PER_KEY = {
     ("group", 512): {"alu": 3298, "inst": 5826, "dram_bytes": 31.6},
-    ("group", 256): {"alu": 3352, "inst": 5878, "dram_bytes": 28.6},
+    ("group", 256): {"alu": 3348, "inst": 5936, "dram_bytes": 31.1},
     ("xadd", 128): {"alu": 4282, "inst": 8093, "dram_bytes": 131.9},
 }
 
