@@ -47,11 +47,14 @@ __device__ __forceinline__ fe fe_one() {
 }
 
 // a + b; a carry out of 2^256 is worth 38, and a second carry can only leave
-// a value below 76, so the last fold needs no chain.
+// a value below 76, so the last fold needs no chain.  Adding 38 to limb 0
+// carries into limb 1 with probability below 2^-26 on uniform inputs, so that
+// chain is a branch: the common case skips seven carry steps.
 __device__ __forceinline__ fe fe_add(const fe& a, const fe& b) {
     fe o;
     asm("{\n\t"
         ".reg .u32 c, t;\n\t"
+        ".reg .pred p;\n\t"
         "add.cc.u32 %0, %8, %16;\n\t"
         "addc.cc.u32 %1, %9, %17;\n\t"
         "addc.cc.u32 %2, %10, %18;\n\t"
@@ -63,7 +66,10 @@ __device__ __forceinline__ fe fe_add(const fe& a, const fe& b) {
         "addc.u32 c, 0, 0;\n\t"
         "mul.lo.u32 t, c, 38;\n\t"
         "add.cc.u32 %0, %0, t;\n\t"
-        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "setp.eq.u32 p, c, 0;\n\t"
+        "@p bra ADDED;\n\t"
+        "add.cc.u32 %1, %1, 1;\n\t"
         "addc.cc.u32 %2, %2, 0;\n\t"
         "addc.cc.u32 %3, %3, 0;\n\t"
         "addc.cc.u32 %4, %4, 0;\n\t"
@@ -72,6 +78,7 @@ __device__ __forceinline__ fe fe_add(const fe& a, const fe& b) {
         "addc.cc.u32 %7, %7, 0;\n\t"
         "addc.u32 c, 0, 0;\n\t"
         "mad.lo.u32 %0, c, 38, %0;\n\t"
+        "ADDED:\n\t"
         "}"
         : "=r"(o.v[0]), "=r"(o.v[1]), "=r"(o.v[2]), "=r"(o.v[3]), "=r"(o.v[4]), "=r"(o.v[5]), "=r"(o.v[6]),
           "=r"(o.v[7])
@@ -81,11 +88,13 @@ __device__ __forceinline__ fe fe_add(const fe& a, const fe& b) {
 }
 
 // a - b; a borrow past 0 added 2^256 = 38, so 38 is taken off again (twice
-// at most: after a second borrow the value is at least 2^256 - 38).
+// at most: after a second borrow the value is at least 2^256 - 38).  As in
+// fe_add, the borrow out of limb 0 is rare and its chain is a branch.
 __device__ __forceinline__ fe fe_sub(const fe& a, const fe& b) {
     fe o;
     asm("{\n\t"
         ".reg .u32 c, t;\n\t"
+        ".reg .pred p;\n\t"
         "sub.cc.u32 %0, %8, %16;\n\t"
         "subc.cc.u32 %1, %9, %17;\n\t"
         "subc.cc.u32 %2, %10, %18;\n\t"
@@ -97,7 +106,10 @@ __device__ __forceinline__ fe fe_sub(const fe& a, const fe& b) {
         "subc.u32 c, 0, 0;\n\t"
         "and.b32 t, c, 38;\n\t"
         "sub.cc.u32 %0, %0, t;\n\t"
-        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 c, 0, 0;\n\t"
+        "setp.eq.u32 p, c, 0;\n\t"
+        "@p bra SUBBED;\n\t"
+        "sub.cc.u32 %1, %1, 1;\n\t"
         "subc.cc.u32 %2, %2, 0;\n\t"
         "subc.cc.u32 %3, %3, 0;\n\t"
         "subc.cc.u32 %4, %4, 0;\n\t"
@@ -107,6 +119,7 @@ __device__ __forceinline__ fe fe_sub(const fe& a, const fe& b) {
         "subc.u32 c, 0, 0;\n\t"
         "and.b32 t, c, 38;\n\t"
         "sub.u32 %0, %0, t;\n\t"
+        "SUBBED:\n\t"
         "}"
         : "=r"(o.v[0]), "=r"(o.v[1]), "=r"(o.v[2]), "=r"(o.v[3]), "=r"(o.v[4]), "=r"(o.v[5]), "=r"(o.v[6]),
           "=r"(o.v[7])

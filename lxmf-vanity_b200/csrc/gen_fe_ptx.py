@@ -20,6 +20,7 @@ def mul_body(square: bool) -> list[str]:
     L = []
     L.append(".reg .u32 r<16>;")
     L.append(".reg .u32 c, c2, t;")
+    L.append(".reg .pred p;")
     if not square:
         # Row 0: r[0..8] = a0 * b.
         L.append(f"mul.lo.u32 r0, {A[0]}, {B[0]};")
@@ -110,14 +111,21 @@ def reduce_lines() -> list[str]:
     for k in range(1, 7):
         L.append(f"madc.hi.cc.u32 r{k + 1}, r{k + 8}, 38, r{k + 1};")
     L.append("madc.hi.u32 c, r15, 38, c;")
-    # value = r0..r7 + c 2^256 with c <= 38: fold c once more.
+    # value = r0..r7 + c 2^256 with c <= 38: fold c once more.  The add into
+    # r0 carries into r1 with probability below 2^-21, so that chain is a
+    # branch the common case skips.
     L.append("mul.lo.u32 t, c, 38;")
     L.append("add.cc.u32 r0, r0, t;")
-    for k in range(1, 8):
+    L.append("addc.u32 c2, 0, 0;")
+    L.append("setp.eq.u32 p, c2, 0;")
+    L.append("@p bra FOLDED;")
+    L.append("add.cc.u32 r1, r1, 1;")
+    for k in range(2, 8):
         L.append(f"addc.cc.u32 r{k}, r{k}, 0;")
     L.append("addc.u32 c2, 0, 0;")
     # A carry here leaves r0..r7 < 38 * 39: adding 38 cannot carry.
     L.append("mad.lo.u32 r0, c2, 38, r0;")
+    L.append("FOLDED:")
     for k in range(8):
         L.append(f"mov.u32 %{k}, r{k};")
     return L

@@ -4,13 +4,32 @@ be checked against Python integers on a machine without a GPU.
 
 Only what the blocks use is implemented: mul/mad/madc (.lo/.hi, with and
 without .cc), add/addc, sub/subc (.cc), shf.l.wrap, shl, shr (.u32/.s32),
-and, xor, mov.  CC.CF is the carry (or the borrow, for sub/subc) flag.
+and, xor, mov, setp.eq.u32, and a predicated (@p / @!p) bra to a label of
+the same block.  CC.CF is the carry (or the borrow, for sub/subc) flag.
 """
 from __future__ import annotations
 
 import re
 
 M32 = 0xFFFFFFFF
+
+
+def _first_colon_outside_strings(asm: str) -> int:
+    """Where the template ends: the first ':' not inside a string literal (a
+    label inside the template has one of its own)."""
+    in_str = False
+    i = 0
+    while i < len(asm):
+        ch = asm[i]
+        if in_str and ch == "\\":
+            i += 2
+            continue
+        if ch == '"':
+            in_str = not in_str
+        elif ch == ":" and not in_str:
+            return i
+        i += 1
+    return len(asm)
 
 
 def extract_asm_blocks(src: str) -> dict[str, tuple[list[str], int]]:
@@ -21,7 +40,7 @@ def extract_asm_blocks(src: str) -> dict[str, tuple[list[str], int]]:
         if "asm(" not in body:
             continue
         asm = body[body.index("asm(") :]
-        head = asm.split(":")[0]
+        head = asm[: _first_colon_outside_strings(asm)]
         strings = re.findall(r'"((?:[^"\\]|\\.)*)"', head)
         text = "".join(strings).replace("\\n", "\n").replace("\\t", " ")
         lines = []
@@ -35,12 +54,16 @@ def extract_asm_blocks(src: str) -> dict[str, tuple[list[str], int]]:
     return out
 
 
-def run(lines: list[str], args: list[int]) -> list[int]:
-    """Execute `lines` with %0.. bound to `args` (outputs first, as zeros)."""
+def run(lines: list[str], args: list[int], branches: dict | None = None) -> list[int]:
+    """Execute `lines` with %0.. bound to `args` (outputs first, as zeros).
+
+    `branches`, when given, counts each bra by (label, taken)."""
     regs: dict[str, int] = {}
+    preds: dict[str, bool] = {}
     for i, v in enumerate(args):
         regs[f"%{i}"] = v & M32
     cf = 0
+    labels = {ln[:-1]: i for i, ln in enumerate(lines) if ln.endswith(":")}
 
     def val(tok: str) -> int:
         tok = tok.strip()
@@ -50,9 +73,32 @@ def run(lines: list[str], args: list[int]) -> list[int]:
             return int(tok, 0) & M32
         raise KeyError(f"undefined operand {tok!r}")
 
-    for ln in lines:
+    pc = 0
+    while pc < len(lines):
+        ln = lines[pc]
+        pc += 1
+        if ln.endswith(":"):
+            continue
+        guard = None
+        if ln.startswith("@"):
+            guard, _, ln = ln.partition(" ")
+            neg = guard.startswith("@!")
+            guard = preds[guard[2:] if neg else guard[1:]] != neg
         op, _, rest = ln.partition(" ")
         ops = [t.strip() for t in rest.split(",")]
+        if op == "bra":
+            assert guard is not None, "only predicated branches are used"
+            if branches is not None:
+                key = (ops[0], guard)
+                branches[key] = branches.get(key, 0) + 1
+            if guard:
+                pc = labels[ops[0]]
+            continue
+        if guard is not None:
+            raise NotImplementedError("predicated " + op)
+        if op == "setp.eq.u32":
+            preds[ops[0]] = val(ops[1]) == val(ops[2])
+            continue
         parts = op.split(".")
         base = parts[0]
         mods = set(parts[1:])

@@ -88,3 +88,24 @@ def test_canon(blocks):
     for a in cases():
         r = call(blocks, "fe_canon", a)
         assert r == a % P, hex(a)
+
+
+@pytest.mark.parametrize("name,label,arity", [("fe_mul_ptx", "FOLDED", 2), ("fe_sqr_ptx", "FOLDED", 1),
+                                              ("fe_add", "ADDED", 2), ("fe_sub", "SUBBED", 2)])
+def test_rare_carry_branch(blocks, name, label, arity):
+    """The last carry (borrow) chain of each block runs only when limb 0
+    carries (borrows); the edge values take both sides, and both give the
+    exact result."""
+    lines, n_out = blocks[name]
+    seen = {}
+    for a in EDGE:
+        for b in (EDGE if arity == 2 else [None]):
+            ins = (a, b) if arity == 2 else (a,)
+            args = [0] * n_out
+            for x in ins:
+                args += ptx_emu.words(x)
+            r = ptx_emu.value(ptx_emu.run(lines, args, seen)[:8])
+            want = {"fe_mul_ptx": lambda: a * b, "fe_sqr_ptx": lambda: a * a,
+                    "fe_add": lambda: a + b, "fe_sub": lambda: a - b}[name]()
+            assert 0 <= r < 2**256 and r % P == want % P, tuple(hex(x) for x in ins)
+    assert seen.get((label, True), 0) > 0 and seen.get((label, False), 0) > 0, seen
