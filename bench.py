@@ -57,9 +57,9 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
 # profiles/walk_group_g256_plain_search.md, profiles/walk_xadd_b128_plain_search.md):
 # ALU-pipe lane operations (the binding pipe), all instructions, and DRAM bytes (read + write).
 NCU_PER_KEY = {
-    ("group", 512): {"alu": 3298, "inst": 5826, "dram_bytes": 31.6},
-    ("group", 256): {"alu": 3348, "inst": 5936, "dram_bytes": 31.1},
-    ("xadd", 128): {"alu": 4282, "inst": 8093, "dram_bytes": 131.9},
+    ("group", 512): {"alu": 3243, "inst": 5823, "dram_bytes": 31.6},
+    ("group", 256): {"alu": 3288, "inst": 5935, "dram_bytes": 31.1},
+    ("xadd", 128): {"alu": 4166, "inst": 8120, "dram_bytes": 131.9},
 }
 
 
