@@ -293,9 +293,10 @@ int lxmfv_address_of_identity(const uint8_t identity[64], const uint8_t name_has
 
 /* lxmf_address (main.rs:180-189) on `count` 64-byte public keys (x_pub then
  * ed_pub) with one name hash, on this CPU thread: 16-byte outputs.  impl 0:
- * the SHA extensions where present, else portable C; 1: portable C; 2: the x86
- * SHA extensions; 3: the same, two keys at a time as the CPU search hashes
- * them (2 and 3: LXMFV_ERR_STATE where the extensions are absent). */
+ * the fastest this CPU has (4, else 2, else 1); 1: portable C; 2: the x86 SHA
+ * extensions; 3: the same, two keys at a time; 4: AVX-512F, sixteen keys at a
+ * time, as the CPU search hashes them where the CPU has it (2 and 3:
+ * LXMFV_ERR_STATE where the SHA extensions are absent, 4 where AVX-512F is). */
 int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out, int impl);
 
 /* KeyWalk::next_batch (main.rs:255-289) from start scalar k: writes the

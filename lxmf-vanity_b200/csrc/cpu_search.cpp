@@ -7,13 +7,15 @@
 // X25519 keys u(k + 8n), 256 at a time, in walk order (the reference's
 // KeyWalk uses x-only differential addition; here the grouped affine walk of
 // the GPU kernels visits the same keys with a third of the field work); each
-// key's address by the double SHA-256 (cpu_sha256.h: the x86 SHA extensions
-// where present); the first match in walk order is rebuilt from its scalar and
-// rechecked from scratch (OpenSSL) before it is returned.
+// key's address by the double SHA-256 (cpu_sha256.h: 16 keys at a time with
+// AVX-512 where present, else the x86 SHA extensions, else portable C); the
+// first match in walk order is rebuilt from its scalar and rechecked from
+// scratch (OpenSSL) before it is returned.
 // Field: GF(2^255-19) in 5 x 51-bit limbs with 128-bit products.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -26,6 +28,7 @@ namespace {
 typedef unsigned __int128 u128;
 constexpr uint64_t MASK51 = (1ull << 51) - 1;
 constexpr int BATCH = 256;  // keys per batch inversion (a group), as main.rs's BATCH
+static_assert(BATCH % 16 == 0, "keys are hashed 16 at a time");
 
 struct F {
     uint64_t l[5];
@@ -302,11 +305,15 @@ inline bool stopped(const Shared& s) {
            s.error.load(std::memory_order_relaxed) != 0;
 }
 
+// How a walker hashes: portable C, the SHA extensions two keys at a time, or
+// AVX-512 sixteen keys at a time.
+enum Hasher { HASH_C, HASH_NI, HASH_X16 };
+
 // The addresses of two public keys.
-template <bool NI>
+template <Hasher H>
 inline void hash_pair(uint8_t pk[2][64], uint8_t blocks[2][64], uint8_t h[2][16]) {
 #if defined(__x86_64__)
-    if (NI) {
+    if (H == HASH_NI) {
         cpu_sha::address2_ni(pk[0], pk[1], blocks, h[0], h[1]);
         return;
     }
@@ -315,8 +322,19 @@ inline void hash_pair(uint8_t pk[2][64], uint8_t blocks[2][64], uint8_t h[2][16]
     cpu_sha::address<false>(pk[1], blocks[1], h[1]);
 }
 
+// Bit m set where key first + m of `keys` (16 of them) matches the prefix.
+inline uint32_t match16(const uint8_t (*keys)[32], const uint8_t* ed_pub, const uint8_t* nh, const uint32_t want[4],
+                        const uint32_t mask[4]) {
+#if defined(__x86_64__)
+    return cpu_sha::x16::match16(keys[0], 32, ed_pub, nh, want, mask);
+#else
+    (void)keys, (void)ed_pub, (void)nh, (void)want, (void)mask;
+    return 0;
+#endif
+}
+
 // One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed `ed_seed`.
-template <bool NI>
+template <Hasher H>
 void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     uint8_t ed_pub[32];
     Walk w;
@@ -331,17 +349,29 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
         memcpy(pk[j] + 32, ed_pub, 32);
         cpu_sha::address_block(s->nh, blocks[j]);
     }
+    uint32_t want[4], mask[4];
+    lxmfv_prefix_words(s->prefix, s->nibbles, want, mask);
     while (!stopped(*s)) {
         const uint64_t first = w.batch(keys, BATCH);
+        uint32_t hits16 = 0;
         for (int i = 0; i < BATCH; i++) {
-            // Keys are hashed in pairs (two SHA-256 streams interleaved where the
-            // CPU has the SHA extensions) and checked in walk order.
-            if ((i & 1) == 0) {
-                memcpy(pk[0], keys[i], 32);
-                memcpy(pk[1], keys[i + 1], 32);
-                hash_pair<NI>(pk, blocks, h);
+            // Keys are hashed sixteen at a time (AVX-512: a bit per matching
+            // key) or in pairs (two SHA-256 streams interleaved where the CPU
+            // has the SHA extensions), and checked in walk order.
+            if (H == HASH_X16) {
+                if ((i & 15) == 0) hits16 = match16(keys + i, ed_pub, s->nh, want, mask);
+                if (!(hits16 >> (i & 15) & 1)) {
+                    if (!(hits16 >> (i & 15))) i |= 15;  // no match left in these 16
+                    continue;
+                }
+            } else {
+                if ((i & 1) == 0) {
+                    memcpy(pk[0], keys[i], 32);
+                    memcpy(pk[1], keys[i + 1], 32);
+                    hash_pair<H>(pk, blocks, h);
+                }
+                if (!lxmfv_prefix_matches(s->prefix, s->nibbles, h[i & 1])) continue;
             }
-            if (!lxmfv_prefix_matches(s->prefix, s->nibbles, h[i & 1])) continue;
             uint8_t ident[64], addr[16];
             lxmfv_step_scalar(start, first + (uint64_t)i, ident);
             memcpy(ident + 32, ed_seed, 32);
@@ -368,13 +398,36 @@ bool use_sha_ni() {
 #endif
 }
 
+bool use_x16() {
+#if defined(__x86_64__)
+    return cpu_sha::x16::available();
+#else
+    return false;
+#endif
+}
+
 }  // namespace
 
 extern "C" int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out,
                                    int impl) {
-    if ((count && (!pks || !out)) || !name_hash || impl < 0 || impl > 3) return LXMFV_ERR_ARG;
-    if (impl >= 2 && !use_sha_ni()) return LXMFV_ERR_STATE;
+    if ((count && (!pks || !out)) || !name_hash || impl < 0 || impl > 4) return LXMFV_ERR_ARG;
+    if ((impl == 2 || impl == 3) && !use_sha_ni()) return LXMFV_ERR_STATE;
+    if (impl == 4 && !use_x16()) return LXMFV_ERR_STATE;
+    if (impl == 0 && use_x16()) impl = 4;
 #if defined(__x86_64__)
+    if (impl == 4) {
+        uint64_t i = 0;
+        for (; i + 16 <= count; i += 16)
+            cpu_sha::x16::address16_bytes(pks + 64 * i, 64, pks + 64 * i + 32, 64, name_hash, out + 16 * i);
+        if (i < count) {
+            // The last keys, padded to 16 with copies of the final one.
+            uint8_t tail[16][64], addrs[16][16];
+            for (int m = 0; m < 16; m++) memcpy(tail[m], pks + 64 * std::min<uint64_t>(i + m, count - 1), 64);
+            cpu_sha::x16::address16_bytes(tail[0], 64, tail[0] + 32, 64, name_hash, addrs[0]);
+            memcpy(out + 16 * i, addrs, 16 * (size_t)(count - i));
+        }
+        return LXMFV_OK;
+    }
     if (impl == 3) {
         uint8_t blocks[2][64];
         cpu_sha::address_block(name_hash, blocks[0]);
@@ -462,9 +515,21 @@ extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uin
     s.identity_out = identity;
     std::vector<std::thread> pool;
     pool.reserve((size_t)threads);
-    const bool ni = use_sha_ni();
-    for (int t = 0; t < threads; t++)
-        pool.emplace_back(ni ? walker<true> : walker<false>, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
+    // The fastest hasher this CPU has; LXMFV_CPU_HASH=c|ni|x16 picks one (tests
+    // run each), LXMFV_ERR_STATE where the CPU lacks it.
+    void (*run)(Shared*, const uint8_t*, const uint8_t*) =
+        use_x16() ? walker<HASH_X16> : use_sha_ni() ? walker<HASH_NI> : walker<HASH_C>;
+    if (const char* force = getenv("LXMFV_CPU_HASH")) {
+        if (!strcmp(force, "c"))
+            run = walker<HASH_C>;
+        else if (!strcmp(force, "ni") && use_sha_ni())
+            run = walker<HASH_NI>;
+        else if (!strcmp(force, "x16") && use_x16())
+            run = walker<HASH_X16>;
+        else
+            return LXMFV_ERR_STATE;
+    }
+    for (int t = 0; t < threads; t++) pool.emplace_back(run, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
     while (!stopped(s)) {
         if (tries) __atomic_store_n(tries, s.tries.load(std::memory_order_relaxed), __ATOMIC_RELAXED);
         std::this_thread::sleep_for(std::chrono::milliseconds(10));

@@ -1,8 +1,9 @@
 // SHA-256 (FIPS 180-4) for the CPU search's two fixed-size messages: the
 // 64-byte public key (two blocks, the second the constant padding) and the
-// 26-byte name hash || identity hash (one block).  Two compressions: the x86
-// SHA extensions (sha256rnds2 / sha256msg1 / sha256msg2) where the CPU has
-// them, chosen once at run time, else portable C.
+// 26-byte name hash || identity hash (one block).  Three implementations,
+// chosen at run time: AVX-512F sixteen messages at a time (namespace x16),
+// the x86 SHA extensions (sha256rnds2 / sha256msg1 / sha256msg2), one or two
+// messages at a time, and portable C.
 #pragma once
 
 #include <cstdint>
@@ -235,5 +236,192 @@ inline void address_block(const uint8_t nh[10], uint8_t block[64]) {
     block[62] = 0x00;
     block[63] = 208;  // 26 bytes = 208 bits
 }
+
+// K[i] + W[i] of the 64-byte message's padding block, whose schedule is a
+// constant (0x80000000, zeros, bit length 512).
+struct PadKW {
+    uint32_t kw[64];
+    constexpr PadKW() : kw() {
+        uint32_t w[64] = {};
+        w[0] = 0x80000000u;
+        w[15] = 512;
+        for (int i = 16; i < 64; i++) {
+            const uint32_t x = w[i - 15], y = w[i - 2];
+            const uint32_t s0 = ((x >> 7) | (x << 25)) ^ ((x >> 18) | (x << 14)) ^ (x >> 3);
+            const uint32_t s1 = ((y >> 17) | (y << 15)) ^ ((y >> 19) | (y << 13)) ^ (y >> 10);
+            w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+        }
+        for (int i = 0; i < 64; i++) kw[i] = K[i] + w[i];
+    }
+};
+constexpr PadKW PAD_KW{};
+
+#if defined(__x86_64__)
+// Sixteen addresses at once with AVX-512F: message m in 32-bit lane m of each
+// vector.  A rotate is one vprord, and Sigma0 / Sigma1 / sigma0 / sigma1's
+// three-way XOR, Ch and Maj are one vpternlogd each, so a round is about 16
+// vector instructions for 16 keys.
+namespace x16 {
+
+typedef __m512i V;
+#define LXCPU_X16 __attribute__((target("avx512f")))
+
+LXCPU_X16 inline V add(V a, V b) { return _mm512_add_epi32(a, b); }
+LXCPU_X16 inline V xor3(V a, V b, V c) { return _mm512_ternarylogic_epi32(a, b, c, 0x96); }
+LXCPU_X16 inline V bsig0(V a) { return xor3(_mm512_ror_epi32(a, 2), _mm512_ror_epi32(a, 13), _mm512_ror_epi32(a, 22)); }
+LXCPU_X16 inline V bsig1(V e) { return xor3(_mm512_ror_epi32(e, 6), _mm512_ror_epi32(e, 11), _mm512_ror_epi32(e, 25)); }
+LXCPU_X16 inline V ssig0(V w) { return xor3(_mm512_ror_epi32(w, 7), _mm512_ror_epi32(w, 18), _mm512_srli_epi32(w, 3)); }
+LXCPU_X16 inline V ssig1(V w) { return xor3(_mm512_ror_epi32(w, 17), _mm512_ror_epi32(w, 19), _mm512_srli_epi32(w, 10)); }
+LXCPU_X16 inline V ch(V e, V f, V g) { return _mm512_ternarylogic_epi32(e, f, g, 0xCA); }   // e ? f : g
+LXCPU_X16 inline V maj(V a, V b, V c) { return _mm512_ternarylogic_epi32(a, b, c, 0xE8); }  // majority
+// Big-endian word of four little-endian bytes: bytes 3 and 1 from the rotate
+// right by 8, bytes 2 and 0 from the rotate left.
+LXCPU_X16 inline V bswap(V x) {
+    return _mm512_ternarylogic_epi32(_mm512_ror_epi32(x, 8), _mm512_rol_epi32(x, 8), _mm512_set1_epi32((int)0xFF00FF00),
+                                     0xE4);
+}
+
+// One round; the new e lands in d and the new a in h (the caller rotates names).
+#define LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, kw)                 \
+    {                                                              \
+        const V t1_ = add(add(h, kw), add(bsig1(e), ch(e, f, g))); \
+        d = add(d, t1_);                                           \
+        h = add(t1_, add(bsig0(a), maj(a, b, c)));                 \
+    }
+
+// One compression of the 16-word blocks w (schedule extended in place).
+LXCPU_X16 inline void compress(V s[8], V w[16]) {
+    V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
+#pragma GCC unroll 8
+    for (int r = 0; r < 64; r += 8) {
+        if (r >= 16) {
+#pragma GCC unroll 8
+            for (int j = 0; j < 8; j++) {
+                const int i = (r + j) & 15;
+                w[i] = add(add(w[i], ssig0(w[(i + 1) & 15])), add(w[(i + 9) & 15], ssig1(w[(i + 14) & 15])));
+            }
+        }
+        const int q = r & 15;
+        LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, add(w[q + 0], _mm512_set1_epi32((int)K[r + 0])));
+        LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, add(w[q + 1], _mm512_set1_epi32((int)K[r + 1])));
+        LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, add(w[q + 2], _mm512_set1_epi32((int)K[r + 2])));
+        LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, add(w[q + 3], _mm512_set1_epi32((int)K[r + 3])));
+        LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, add(w[q + 4], _mm512_set1_epi32((int)K[r + 4])));
+        LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, add(w[q + 5], _mm512_set1_epi32((int)K[r + 5])));
+        LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, add(w[q + 6], _mm512_set1_epi32((int)K[r + 6])));
+        LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, add(w[q + 7], _mm512_set1_epi32((int)K[r + 7])));
+    }
+    s[0] = add(s[0], a);
+    s[1] = add(s[1], b);
+    s[2] = add(s[2], c);
+    s[3] = add(s[3], d);
+    s[4] = add(s[4], e);
+    s[5] = add(s[5], f);
+    s[6] = add(s[6], g);
+    s[7] = add(s[7], h);
+}
+
+// The padding block's compression: its K + W are the constants PAD_KW.
+LXCPU_X16 inline void compress_pad64(V s[8]) {
+    V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
+#pragma GCC unroll 8
+    for (int r = 0; r < 64; r += 8) {
+        LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, _mm512_set1_epi32((int)PAD_KW.kw[r + 0]));
+        LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, _mm512_set1_epi32((int)PAD_KW.kw[r + 1]));
+        LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, _mm512_set1_epi32((int)PAD_KW.kw[r + 2]));
+        LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, _mm512_set1_epi32((int)PAD_KW.kw[r + 3]));
+        LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, _mm512_set1_epi32((int)PAD_KW.kw[r + 4]));
+        LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, _mm512_set1_epi32((int)PAD_KW.kw[r + 5]));
+        LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, _mm512_set1_epi32((int)PAD_KW.kw[r + 6]));
+        LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, _mm512_set1_epi32((int)PAD_KW.kw[r + 7]));
+    }
+    s[0] = add(s[0], a);
+    s[1] = add(s[1], b);
+    s[2] = add(s[2], c);
+    s[3] = add(s[3], d);
+    s[4] = add(s[4], e);
+    s[5] = add(s[5], f);
+    s[6] = add(s[6], g);
+    s[7] = add(s[7], h);
+}
+#undef LXCPU_X16_ROUND
+
+// The first four big-endian words of the addresses of 16 public keys.  Key m's
+// x_pub is the 32 bytes at x + m * x_stride; its ed_pub the 32 bytes at
+// ed + m * ed_stride (ed_stride 0: one ed_pub for all).  nh: the name hash.
+LXCPU_X16 inline void address16(const uint8_t* x, int x_stride, const uint8_t* ed, int ed_stride, const uint8_t nh[10],
+                                V out[4]) {
+    const V lane = _mm512_set_epi32(15, 14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0);
+    const V xoff = _mm512_mullo_epi32(lane, _mm512_set1_epi32(x_stride));
+    V w[16], s[8];
+    for (int j = 0; j < 8; j++) w[j] = bswap(_mm512_i32gather_epi32(xoff, (const void*)(x + 4 * j), 1));
+    if (ed_stride) {
+        const V eoff = _mm512_mullo_epi32(lane, _mm512_set1_epi32(ed_stride));
+        for (int j = 0; j < 8; j++) w[8 + j] = bswap(_mm512_i32gather_epi32(eoff, (const void*)(ed + 4 * j), 1));
+    } else {
+        for (int j = 0; j < 8; j++) {
+            const uint8_t* p = ed + 4 * j;
+            w[8 + j] = _mm512_set1_epi32((int)((uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]));
+        }
+    }
+    for (int i = 0; i < 8; i++) s[i] = _mm512_set1_epi32((int)IV[i]);
+    compress(s, w);
+    compress_pad64(s);
+    // Second hash: name_hash (10 bytes) || identity hash (16 bytes), 0x80, length 208.
+    const uint32_t nh0 = (uint32_t)nh[0] << 24 | (uint32_t)nh[1] << 16 | (uint32_t)nh[2] << 8 | nh[3];
+    const uint32_t nh1 = (uint32_t)nh[4] << 24 | (uint32_t)nh[5] << 16 | (uint32_t)nh[6] << 8 | nh[7];
+    const uint32_t nh2 = (uint32_t)nh[8] << 24 | (uint32_t)nh[9] << 16;
+    w[0] = _mm512_set1_epi32((int)nh0);
+    w[1] = _mm512_set1_epi32((int)nh1);
+    w[2] = _mm512_or_si512(_mm512_set1_epi32((int)nh2), _mm512_srli_epi32(s[0], 16));
+    w[3] = _mm512_or_si512(_mm512_slli_epi32(s[0], 16), _mm512_srli_epi32(s[1], 16));
+    w[4] = _mm512_or_si512(_mm512_slli_epi32(s[1], 16), _mm512_srli_epi32(s[2], 16));
+    w[5] = _mm512_or_si512(_mm512_slli_epi32(s[2], 16), _mm512_srli_epi32(s[3], 16));
+    w[6] = _mm512_or_si512(_mm512_slli_epi32(s[3], 16), _mm512_set1_epi32(0x8000));
+    for (int j = 7; j < 15; j++) w[j] = _mm512_setzero_si512();
+    w[15] = _mm512_set1_epi32(208);
+    for (int i = 0; i < 8; i++) s[i] = _mm512_set1_epi32((int)IV[i]);
+    compress(s, w);
+    for (int i = 0; i < 4; i++) out[i] = s[i];
+}
+
+// The 16 addresses as bytes: out + 16 * m for key m.
+LXCPU_X16 inline void address16_bytes(const uint8_t* x, int x_stride, const uint8_t* ed, int ed_stride,
+                                      const uint8_t nh[10], uint8_t* out) {
+    V h[4];
+    address16(x, x_stride, ed, ed_stride, nh, h);
+    alignas(64) uint32_t words[4][16];
+    for (int i = 0; i < 4; i++) _mm512_store_si512((void*)words[i], h[i]);
+    for (int m = 0; m < 16; m++)
+        for (int i = 0; i < 4; i++) {
+            out[16 * m + 4 * i] = (uint8_t)(words[i][m] >> 24);
+            out[16 * m + 4 * i + 1] = (uint8_t)(words[i][m] >> 16);
+            out[16 * m + 4 * i + 2] = (uint8_t)(words[i][m] >> 8);
+            out[16 * m + 4 * i + 3] = (uint8_t)words[i][m];
+        }
+}
+
+// Bit m set where key m's address matches: (word[i] & mask[i]) == want[i] for
+// the big-endian prefix words with a nonzero mask (want already masked).
+LXCPU_X16 inline uint32_t match16(const uint8_t* x, int x_stride, const uint8_t* ed, const uint8_t nh[10],
+                                  const uint32_t want[4], const uint32_t mask[4]) {
+    V h[4];
+    address16(x, x_stride, ed, 0, nh, h);
+    __mmask16 m = 0xFFFF;
+    for (int i = 0; i < 4; i++)
+        if (mask[i])
+            m &= _mm512_cmpeq_epi32_mask(_mm512_and_si512(h[i], _mm512_set1_epi32((int)mask[i])),
+                                         _mm512_set1_epi32((int)want[i]));
+    return m;
+}
+
+inline bool available() {
+    static const bool yes = __builtin_cpu_supports("avx512f");
+    return yes;
+}
+
+#undef LXCPU_X16
+}  // namespace x16
+#endif
 
 }  // namespace cpu_sha

@@ -40,7 +40,7 @@ def test_walk_keys_are_x25519_of_the_stepped_scalars(lx):
         assert bytes(keys[n]) == O.x25519_base(O.step_scalar(ident[:32], n))
 
 
-@pytest.mark.parametrize("impl", [0, 1, 2, 3])
+@pytest.mark.parametrize("impl", [0, 1, 2, 3, 4])
 def test_addresses_match_the_oracle(lx, impl):
     rng = np.random.default_rng(impl)
     pks = rng.integers(0, 256, (3000, 64), dtype=np.uint8)
@@ -48,9 +48,25 @@ def test_addresses_match_the_oracle(lx, impl):
         try:
             got = lx.cpu_addresses(pks, aspect, impl=impl)
         except lx.LxmfvError as e:
-            assert impl >= 2 and e.code == lx.ERR_STATE  # no SHA extensions on this CPU
-            pytest.skip("this CPU has no SHA extensions")
+            assert impl >= 2 and e.code == lx.ERR_STATE  # no SHA extensions / AVX-512F on this CPU
+            pytest.skip("this CPU lacks the instructions of this implementation")
         assert np.array_equal(got, O.address_chain(pks, O.name_hash(aspect)))
+
+
+@pytest.mark.parametrize("count", [1, 2, 15, 16, 17, 31, 33])
+def test_addresses_ragged_counts(lx, count):
+    """Counts that are not a multiple of the 16 keys the AVX-512 path hashes
+    at once (its tail is padded), against the portable path and the oracle."""
+    rng = np.random.default_rng(100 + count)
+    pks = rng.integers(0, 256, (count, 64), dtype=np.uint8)
+    want = O.address_chain(pks, O.name_hash("lxmf.propagation"))
+    for impl in (0, 1, 3, 4):
+        try:
+            got = lx.cpu_addresses(pks, "lxmf.propagation", impl=impl)
+        except lx.LxmfvError as e:
+            assert e.code == lx.ERR_STATE
+            continue
+        assert np.array_equal(got, want), impl
 
 
 def test_golden_destination_hashes(lx, config1):
@@ -81,6 +97,34 @@ def test_seeded_walker_matches_the_oracle(lx, walker):
     got = s.run()
     assert got == O.step_scalar(start, int(hits[0])) + ed_seed
     assert s.tries == int(hits[0]) + 1
+
+
+@pytest.mark.parametrize("hasher", ["c", "ni", "x16"])
+@pytest.mark.parametrize("prefix_text", ["c3", "e01"])
+def test_every_hasher_finds_the_first_hit(lx, monkeypatch, hasher, prefix_text):
+    """Each of the search's hashers (portable C, SHA extensions in pairs,
+    AVX-512 sixteen at a time) returns the oracle's first hit in walk order,
+    with the same tries."""
+    monkeypatch.setenv("LXMFV_CPU_HASH", hasher)
+    seed, prefix = 13, O.prefix_parse(prefix_text)
+    k0, ed_seed, _ = O.seeded_identity(seed)
+    hits, _ = O.search_window(k0, O.ed25519_public(ed_seed), O.name_hash(), prefix, 8192)
+    assert len(hits), "the window holds a hit"
+    s = lx.CpuSearch(prefix, threads=1, seed=seed)
+    try:
+        got = s.run()
+    except lx.LxmfvError as e:
+        assert hasher != "c" and e.code == lx.ERR_STATE
+        pytest.skip("this CPU lacks the instructions of this hasher")
+    assert got == O.step_scalar(k0, int(hits[0])) + ed_seed
+    assert s.tries == int(hits[0]) + 1
+
+
+def test_unknown_hasher_is_refused(lx, monkeypatch):
+    monkeypatch.setenv("LXMFV_CPU_HASH", "sha3")
+    with pytest.raises(lx.LxmfvError) as e:
+        lx.CpuSearch(lx.prefix_parse("c3"), threads=1, seed=13).run()
+    assert e.value.code == lx.ERR_STATE
 
 
 def test_many_threads_give_a_valid_identity(lx):
@@ -125,4 +169,4 @@ def test_bad_arguments(lx):
     assert f(pb, 2, nh, 1, None, 5, C.byref(stop), C.byref(tries), ident) == lx.ERR_ARG   # walker without seed
     assert f(pb, 2, nh, 1, None, 0, None, C.byref(tries), ident) == lx.ERR_ARG            # no stop flag
     assert lx.lib().lxmfv_cpu_walk(None, 4, None) == lx.ERR_ARG
-    assert lx.lib().lxmfv_cpu_addresses(None, 0, nh, None, 4) == lx.ERR_ARG
+    assert lx.lib().lxmfv_cpu_addresses(None, 0, nh, None, 5) == lx.ERR_ARG
