@@ -177,7 +177,8 @@ def cpu_search_rate(seconds: float = 3.0) -> dict:
     dt = time.perf_counter() - t0
     return {"value": s.tries / dt, "unit": "keys/s", "threads": threads, "seconds": round(dt, 2),
             "found": found is not None,
-            "api": "lxmfv_cpu_search (grouped affine walk, 5 x 51-bit field; SHA-256 16 keys at a time with AVX-512F, else the x86 SHA extensions, else portable C)"}
+            "api": "lxmfv_cpu_search (grouped affine walk, 5 x 51-bit field on 8 AVX-512 IFMA lanes where "
+                   "present; SHA-256 16 keys at a time with AVX-512F, else the x86 SHA extensions, else portable C)"}
 
 
 def reference_cpu(prefix: str, steps: int, warmup: int, step_seconds: float = 2.0) -> dict:

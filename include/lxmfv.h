@@ -300,7 +300,10 @@ int lxmfv_address_of_identity(const uint8_t identity[64], const uint8_t name_has
 int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uint8_t name_hash[10], uint8_t* out, int impl);
 
 /* KeyWalk::next_batch (main.rs:255-289) from start scalar k: writes the
- * X25519 public keys u(k + 8n), n = 0 .. count-1, 32 bytes each. */
+ * X25519 public keys u(k + 8n), n = 0 .. count-1, 32 bytes each.  It and
+ * lxmfv_cpu_search walk on eight AVX-512 IFMA lanes where the CPU has them,
+ * else in scalar 64-bit code; the environment variable LXMFV_CPU_WALK=scalar
+ * or =ifma picks one (LXMFV_ERR_STATE where it is unavailable or unknown). */
 int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys);
 
 /* search on `threads` CPU threads (main.rs:292-323, fanned out as
@@ -312,7 +315,10 @@ int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys);
  * scalar draw, first_walker <= 2^24) with the identity's Ed25519 seed.
  * *tries (may be NULL) is updated every 10 ms with the keys tried.  Writes
  * the rechecked 64-byte identity and returns LXMFV_OK; LXMFV_STOPPED when
- * stopped without a hit; LXMFV_ERR_RECHECK when a hit failed its recheck. */
+ * stopped without a hit; LXMFV_ERR_RECHECK when a hit failed its recheck.
+ * LXMFV_CPU_HASH=c, =ni or =x16 picks the SHA-256 code (portable C, the SHA
+ * extensions, AVX-512F) instead of the fastest; LXMFV_ERR_STATE where the
+ * CPU lacks it. */
 int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
                      const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
                      uint8_t identity[64]);

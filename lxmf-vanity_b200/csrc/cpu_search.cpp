@@ -4,19 +4,23 @@
 // search; the GPU entry points never fall back to it.
 //
 // Per thread, as the reference: one start scalar k and one Ed25519 seed; the
-// X25519 keys u(k + 8n), 256 at a time, in walk order (the reference's
+// X25519 keys u(k + 8n) in walk order, a group at a time (the reference's
 // KeyWalk uses x-only differential addition; here the grouped affine walk of
-// the GPU kernels visits the same keys with a third of the field work); each
+// the GPU kernels visits the same keys with a third of the field work: 2048
+// keys per group on eight AVX-512 IFMA lanes where the CPU has them, else 256
+// per group in scalar code); each
 // key's address by the double SHA-256 (cpu_sha256.h: 16 keys at a time with
 // AVX-512 where present, else the x86 SHA extensions, else portable C); the
 // first match in walk order is rebuilt from its scalar and rechecked from
 // scratch (OpenSSL) before it is returned.
-// Field: GF(2^255-19) in 5 x 51-bit limbs with 128-bit products.
+// Field: GF(2^255-19) in 5 x 51-bit limbs, with 128-bit products (scalar) or
+// 52-bit multiply-adds (IFMA lanes).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -172,8 +176,9 @@ void add_affine(const F& u1, const F& v1, const F& u2, const F& v2, F& u3, F& v3
 
 // The group table: T_i = i Q (i = 1..M) and T_0 = J = 2M Q, affine, with
 // Q = 8B = (u(8B), v(8B)); built once by affine additions.
+template <int M>
 struct GroupTable {
-    F u[HALF + 1], v[HALF + 1];
+    F u[M + 1], v[M + 1];
     GroupTable() {
         const F uq = from_bytes(U8B_BYTES), vq = from_words(V8B_WORDS);
         // T_2 = 2Q by the tangent: l = (3u^2 + 2Au + 1) / 2v.
@@ -184,12 +189,12 @@ struct GroupTable {
         v[1] = vq;
         u[2] = tu;
         v[2] = tv;
-        for (int i = 3; i <= 2 * HALF; i++) {
+        for (int i = 3; i <= 2 * M; i++) {
             F nu, nv;
             add_affine(tu, tv, uq, vq, nu, nv);
             tu = nu;
             tv = nv;
-            if (i <= HALF) {
+            if (i <= M) {
                 u[i] = tu;
                 v[i] = tv;
             }
@@ -199,9 +204,38 @@ struct GroupTable {
     }
 };
 
-const GroupTable& group_table() {
-    static const GroupTable t;  // thread-safe initialisation (C++11)
+template <int M>
+const GroupTable<M>& group_table() {
+    static const GroupTable<M> t;  // thread-safe initialisation (C++11)
     return t;
+}
+
+// P = kB in affine coordinates from u(k - 8) and u(k): Okeya-Sakurai y
+// recovery with -Q, since P - Q is the known neighbour.
+int start_point(const uint8_t k[32], F& pu, F& pv) {
+    uint8_t prev[32], b[32];
+    lxmfv_previous_scalar(k, prev);
+    if (lxmfv_x25519_base(prev, b) != LXMFV_OK) return LXMFV_ERR_STATE;
+    const F um8 = from_bytes(b);
+    if (lxmfv_x25519_base(k, b) != LXMFV_OK) return LXMFV_ERR_STATE;
+    const F uk = from_bytes(b);
+    const F xp = from_bytes(U8B_BYTES), yp = sub(F{{0, 0, 0, 0, 0}}, from_words(V8B_WORDS));
+    // recover_y with (X1:Z1) = (uk:1), (X2:Z2) = (um8:1)
+    F v1 = xp;
+    F v2 = add(uk, v1);
+    F v3 = sub(uk, v1);
+    v3 = mul(sqr(v3), um8);
+    v1 = small(2 * 486662);
+    v2 = add(v2, v1);
+    const F v4 = add(mul(xp, uk), ONE);
+    v2 = mul(v2, v4);
+    v2 = sub(v2, v1);
+    const F Y = sub(v2, v3);
+    const F c = add(yp, yp);
+    const F zi = invert(c);
+    pu = uk;
+    pv = mul(Y, zi);  // X = c uk, Z = c: u = uk
+    return LXMFV_OK;
 }
 
 // u(k + 8n) for n = 0, 1, 2, ... by the grouped affine walk, the same keys as
@@ -214,31 +248,13 @@ struct Walk {
     uint64_t next = 0;
     uint8_t buf[BATCH][32];
 
+    static constexpr int SIZE = BATCH;
+
+    // The walk from scalar k: the first group's centre C = P + M Q.
     int init(const uint8_t k[32]) {
-        // y of P = kB = (k/8) Q from u(k - 8) and u(k) (Okeya-Sakurai recovery
-        // with -Q, since P - Q is the known neighbour), then C = P + M Q.
-        uint8_t prev[32], b[32];
-        lxmfv_previous_scalar(k, prev);
-        if (lxmfv_x25519_base(prev, b) != LXMFV_OK) return LXMFV_ERR_STATE;
-        const F um8 = from_bytes(b);
-        if (lxmfv_x25519_base(k, b) != LXMFV_OK) return LXMFV_ERR_STATE;
-        const F uk = from_bytes(b);
-        const F xp = from_bytes(U8B_BYTES), yp = sub(F{{0, 0, 0, 0, 0}}, from_words(V8B_WORDS));
-        // recover_y with (X1:Z1) = (uk:1), (X2:Z2) = (um8:1)
-        F v1 = xp;
-        F v2 = add(uk, v1);
-        F v3 = sub(uk, v1);
-        v3 = mul(sqr(v3), um8);
-        v1 = small(2 * 486662);
-        v2 = add(v2, v1);
-        const F v4 = add(mul(xp, uk), ONE);
-        v2 = mul(v2, v4);
-        v2 = sub(v2, v1);
-        const F Y = sub(v2, v3);
-        const F c = add(yp, yp);
-        const F zi = invert(c);
-        const F pu = uk, pv = mul(Y, zi);  // X = c uk, Z = c: u = uk
-        const GroupTable& t = group_table();
+        F pu, pv;
+        if (int rc = start_point(k, pu, pv)) return rc;
+        const GroupTable<HALF>& t = group_table<HALF>();
         add_affine(pu, pv, t.u[HALF], t.v[HALF], uc, vc);
         next = 0;
         return LXMFV_OK;
@@ -246,7 +262,7 @@ struct Walk {
 
     // The group of keys next .. next + BATCH - 1 into buf, in walk order.
     void group() {
-        const GroupTable& t = group_table();
+        const GroupTable<HALF>& t = group_table<HALF>();
         F pre[HALF + 1];
         F acc = sub(t.u[0], uc);
         for (int i = 1; i <= HALF; i++) {
@@ -279,16 +295,274 @@ struct Walk {
         vc = vnext;
     }
 
-    // The next `len` <= BATCH keys (a whole group; a shorter request keeps its
-    // first keys and ends the walk); returns the walk index of the first.
-    uint64_t batch(uint8_t (*out)[32], int len) {
+    // The next group's SIZE keys in walk order; *first: the walk index of the first.
+    const uint8_t (*next_group(uint64_t* first))[32] {
         group();
-        memcpy(out, buf, 32 * (size_t)len);
-        const uint64_t first = next;
-        next += BATCH;
-        return first;
+        *first = next;
+        next += SIZE;
+        return buf;
     }
 };
+
+#if defined(__x86_64__)
+// The same walk with the field work on eight lanes of AVX-512 IFMA (52-bit
+// multiply-add): GF(2^255-19) in the same 5 x 51-bit limbs, one walker's
+// group elements spread over the lanes.  Groups are 2048 keys (M = 1024), so
+// that the one scalar inversion per group costs about 1/8 of a multiply per
+// key.
+namespace ifma {
+
+#define LXCPU_IFMA __attribute__((target("avx512f,avx512ifma")))
+
+constexpr int M = 1024;      // a group is the 2M keys around one centre
+constexpr int ROWS = M / 8;  // group elements per lane: lane j holds i = 1 + j + 8r
+
+// Eight field elements, limb-major: l[k] holds limb k of lanes 0..7.  Every
+// operation returns limbs below 2^52 (the multiplier reads 52 bits).
+struct alignas(64) Lanes {
+    uint64_t l[5][8];
+};
+
+struct Table {
+    Lanes u[ROWS], v[ROWS];  // T_i = iQ, i = 1..M, lane-major
+    F u0, v0, uM, vM;        // T_0 = J = 2M Q and T_M
+    Table() {
+        const GroupTable<M>& t = group_table<M>();
+        for (int r = 0; r < ROWS; r++)
+            for (int j = 0; j < 8; j++)
+                for (int k = 0; k < 5; k++) {
+                    u[r].l[k][j] = t.u[1 + j + 8 * r].l[k];
+                    v[r].l[k][j] = t.v[1 + j + 8 * r].l[k];
+                }
+        u0 = t.u[0];
+        v0 = t.v[0];
+        uM = t.u[M];
+        vM = t.v[M];
+    }
+};
+
+const Table& table() {
+    static const Table t;
+    return t;
+}
+
+typedef __m512i V;
+struct FV {
+    V l[5];
+};
+
+LXCPU_IFMA inline FV load(const Lanes& a) {
+    FV r;
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_load_si512((const void*)a.l[k]);
+    return r;
+}
+LXCPU_IFMA inline void store(Lanes& a, const FV& x) {
+    for (int k = 0; k < 5; k++) _mm512_store_si512((void*)a.l[k], x.l[k]);
+}
+LXCPU_IFMA inline FV bcast(const F& a) {
+    FV r;
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_set1_epi64((long long)a.l[k]);
+    return r;
+}
+LXCPU_IFMA inline V times19(V x) { return _mm512_add_epi64(_mm512_add_epi64(_mm512_slli_epi64(x, 4), _mm512_slli_epi64(x, 1)), x); }
+
+// As the scalar carry: limbs below 2^63 in, limb 1 at most 2^51 and the
+// others below 2^51 out.
+LXCPU_IFMA inline FV carry(FV a) {
+    const V m = _mm512_set1_epi64((long long)MASK51);
+    for (int i = 0; i < 4; i++) {
+        a.l[i + 1] = _mm512_add_epi64(a.l[i + 1], _mm512_srli_epi64(a.l[i], 51));
+        a.l[i] = _mm512_and_si512(a.l[i], m);
+    }
+    const V c = _mm512_srli_epi64(a.l[4], 51);
+    a.l[4] = _mm512_and_si512(a.l[4], m);
+    a.l[0] = _mm512_add_epi64(a.l[0], times19(c));
+    a.l[1] = _mm512_add_epi64(a.l[1], _mm512_srli_epi64(a.l[0], 51));
+    a.l[0] = _mm512_and_si512(a.l[0], m);
+    return a;
+}
+
+LXCPU_IFMA inline FV add(const FV& a, const FV& b) {
+    FV r;
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(a.l[k], b.l[k]);
+    return carry(r);
+}
+
+// a - b + 4p, as the scalar sub.
+LXCPU_IFMA inline FV sub(const FV& a, const FV& b) {
+    FV r;
+    r.l[0] = _mm512_sub_epi64(_mm512_add_epi64(a.l[0], _mm512_set1_epi64((long long)(4 * (MASK51 - 18)))), b.l[0]);
+    for (int k = 1; k < 5; k++)
+        r.l[k] = _mm512_sub_epi64(_mm512_add_epi64(a.l[k], _mm512_set1_epi64((long long)(4 * MASK51))), b.l[k]);
+    return carry(r);
+}
+
+// a * b mod p.  A 52 x 52-bit product splits at bit 52: its low half goes to
+// column i + j and its high half, worth 2^52 = 2 * 2^51, to column i + j + 1
+// doubled (the high halves are summed apart and doubled once).  Columns 5..9
+// fold down with 2^255 = 19.  Column bounds: 5 low + 10 high halves < 2^56;
+// after the fold below 2^62.
+LXCPU_IFMA inline FV mul(const FV& a, const FV& b) {
+    V lo[10], hi[10];
+    for (int k = 0; k < 10; k++) lo[k] = hi[k] = _mm512_setzero_si512();
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            lo[i + j] = _mm512_madd52lo_epu64(lo[i + j], a.l[i], b.l[j]);
+            hi[i + j + 1] = _mm512_madd52hi_epu64(hi[i + j + 1], a.l[i], b.l[j]);
+        }
+    for (int k = 1; k < 10; k++) lo[k] = _mm512_add_epi64(lo[k], _mm512_slli_epi64(hi[k], 1));
+    FV r;
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(lo[k], times19(lo[k + 5]));
+    return carry(r);
+}
+
+// a^2: the cross products once, doubled.
+LXCPU_IFMA inline FV sqr(const FV& a) {
+    V lo[10], hi[10], xlo[10], xhi[10];
+    for (int k = 0; k < 10; k++) lo[k] = hi[k] = xlo[k] = xhi[k] = _mm512_setzero_si512();
+    for (int i = 0; i < 5; i++) {
+        lo[2 * i] = _mm512_madd52lo_epu64(lo[2 * i], a.l[i], a.l[i]);
+        hi[2 * i + 1] = _mm512_madd52hi_epu64(hi[2 * i + 1], a.l[i], a.l[i]);
+        for (int j = i + 1; j < 5; j++) {
+            xlo[i + j] = _mm512_madd52lo_epu64(xlo[i + j], a.l[i], a.l[j]);
+            xhi[i + j + 1] = _mm512_madd52hi_epu64(xhi[i + j + 1], a.l[i], a.l[j]);
+        }
+    }
+    // column k = lo + 2 hi + 2 xlo + 4 xhi
+    for (int k = 0; k < 10; k++)
+        lo[k] = _mm512_add_epi64(_mm512_add_epi64(lo[k], _mm512_slli_epi64(xlo[k], 1)),
+                                 _mm512_slli_epi64(_mm512_add_epi64(hi[k], _mm512_slli_epi64(xhi[k], 1)), 1));
+    FV r;
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(lo[k], times19(lo[k + 5]));
+    return carry(r);
+}
+
+// The canonical encodings of the eight lanes as four little-endian 64-bit
+// words each (w[i] lane j), as the scalar to_bytes.
+LXCPU_IFMA inline void to_words(FV a, V w[4]) {
+    a = carry(a);
+    const V m = _mm512_set1_epi64((long long)MASK51);
+    V q = _mm512_srli_epi64(_mm512_add_epi64(a.l[0], _mm512_set1_epi64(19)), 51);
+    for (int i = 1; i < 5; i++) q = _mm512_srli_epi64(_mm512_add_epi64(a.l[i], q), 51);
+    a.l[0] = _mm512_add_epi64(a.l[0], times19(q));
+    for (int i = 0; i < 4; i++) {
+        a.l[i + 1] = _mm512_add_epi64(a.l[i + 1], _mm512_srli_epi64(a.l[i], 51));
+        a.l[i] = _mm512_and_si512(a.l[i], m);
+    }
+    a.l[4] = _mm512_and_si512(a.l[4], m);
+    w[0] = _mm512_or_si512(a.l[0], _mm512_slli_epi64(a.l[1], 51));
+    w[1] = _mm512_or_si512(_mm512_srli_epi64(a.l[1], 13), _mm512_slli_epi64(a.l[2], 38));
+    w[2] = _mm512_or_si512(_mm512_srli_epi64(a.l[2], 26), _mm512_slli_epi64(a.l[3], 25));
+    w[3] = _mm512_or_si512(_mm512_srli_epi64(a.l[3], 39), _mm512_slli_epi64(a.l[4], 12));
+}
+
+// Lane j's encoding into out[rows[j]].
+LXCPU_IFMA inline void store_keys(const FV& a, uint8_t (*out)[32], const int rows[8]) {
+    V w[4];
+    to_words(a, w);
+    alignas(64) uint64_t t[4][8];
+    for (int i = 0; i < 4; i++) _mm512_store_si512((void*)t[i], w[i]);
+    for (int j = 0; j < 8; j++) {
+        if (rows[j] < 0) continue;
+        for (int i = 0; i < 4; i++) memcpy(out[rows[j]] + 8 * i, &t[i][j], 8);
+    }
+}
+
+struct Scratch {
+    Lanes pre[ROWS];  // lane j, row r: the product of its elements before row r
+    Lanes acc;
+    uint8_t buf[2 * M][32];
+};
+
+// One group: scratch->buf gets keys c - M .. c + M - 1 in walk order, and
+// (uc, vc) moves to the next centre C + J.  The denominators u_{T_i} - u_C,
+// i = 1..M, are eight interleaved Montgomery chains (one per lane); their
+// eight totals and T_0's denominator share one scalar inversion.
+LXCPU_IFMA void group(F& uc, F& vc, Scratch* s) {
+    const Table& t = table();
+    const FV UC = bcast(uc), VC = bcast(vc);
+    FV acc = bcast(ONE);
+    for (int r = 0; r < ROWS; r++) {
+        store(s->pre[r], acc);
+        acc = mul(acc, sub(load(t.u[r]), UC));
+    }
+    store(s->acc, acc);
+    // Scalar: d0 = u_J - u_C and the eight lane totals, inverted together.
+    F q[9], run[9];
+    q[0] = ::sub(t.u0, uc);
+    for (int j = 0; j < 8; j++)
+        for (int k = 0; k < 5; k++) q[1 + j].l[k] = s->acc.l[k][j];
+    run[0] = q[0];
+    for (int m = 1; m < 9; m++) run[m] = ::mul(run[m - 1], q[m]);
+    F inv = invert(run[8]);
+    Lanes lane_inv;
+    for (int m = 8; m >= 1; m--) {
+        const F x = ::mul(inv, run[m - 1]);  // 1 / q[m]
+        for (int k = 0; k < 5; k++) lane_inv.l[k][m - 1] = x.l[k];
+        inv = ::mul(inv, q[m]);
+    }
+    const F inv_d0 = inv;
+    const F s0 = ::add(uc, small(486662));
+    const FV S0 = bcast(s0);
+    FV INV = load(lane_inv);
+    for (int r = ROWS - 1; r >= 0; r--) {
+        const FV TU = load(t.u[r]), TV = load(t.v[r]);
+        const FV invi = mul(INV, load(s->pre[r]));  // 1 / (u_{T_i} - u_C)
+        INV = mul(INV, sub(TU, UC));
+        const FV sum = add(S0, TU);
+        const FV lp = mul(sub(TV, VC), invi);
+        const FV lm = mul(add(TV, VC), invi);
+        int rows_m[8], rows_p[8];
+        for (int j = 0; j < 8; j++) {
+            const int i = 1 + j + 8 * r;
+            rows_m[j] = M - i;                  // C - T_i: key c - i
+            rows_p[j] = i < M ? M + i : -1;     // C + T_i: key c + i (C + T_M starts the next group)
+        }
+        store_keys(sub(sqr(lm), sum), s->buf, rows_m);
+        store_keys(sub(sqr(lp), sum), s->buf, rows_p);
+    }
+    // T_0 = J: the centre's own key, and the next centre C + J.
+    to_bytes(s->buf[M], uc);
+    const F lp = ::mul(::sub(t.v0, vc), inv_d0);
+    const F up = ::sub(::sqr(lp), ::add(s0, t.u0));
+    vc = ::sub(::mul(lp, ::sub(uc, up)), vc);
+    uc = up;
+}
+
+#undef LXCPU_IFMA
+
+inline bool available() {
+    static const bool yes = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512ifma");
+    return yes;
+}
+
+}  // namespace ifma
+
+// The walk on the IFMA lanes: the same keys as Walk in the same order, in
+// groups of 2048.
+struct WalkIfma {
+    static constexpr int SIZE = 2 * ifma::M;
+    F uc, vc;
+    uint64_t next = 0;
+    std::unique_ptr<ifma::Scratch> s{new ifma::Scratch};
+
+    int init(const uint8_t k[32]) {
+        F pu, pv;
+        if (int rc = start_point(k, pu, pv)) return rc;
+        const ifma::Table& t = ifma::table();
+        add_affine(pu, pv, t.uM, t.vM, uc, vc);
+        next = 0;
+        return LXMFV_OK;
+    }
+
+    const uint8_t (*next_group(uint64_t* first))[32] {
+        ifma::group(uc, vc, s.get());
+        *first = next;
+        next += SIZE;
+        return s->buf;
+    }
+};
+#endif
 
 struct Shared {
     const uint8_t* prefix;
@@ -333,17 +607,18 @@ inline uint32_t match16(const uint8_t (*keys)[32], const uint8_t* ed_pub, const 
 #endif
 }
 
-// One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed `ed_seed`.
-template <Hasher H>
+// One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed
+// `ed_seed`, walking with W (Walk, or WalkIfma on the IFMA lanes).
+template <Hasher H, class W>
 void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     uint8_t ed_pub[32];
-    Walk w;
+    W w;
     if (lxmfv_ed25519_public(ed_seed, ed_pub) != LXMFV_OK || w.init(start) != LXMFV_OK) {
         s->error.store(LXMFV_ERR_STATE);
         return;
     }
-    std::vector<uint8_t> keybuf(BATCH * 32);
-    uint8_t(*keys)[32] = reinterpret_cast<uint8_t(*)[32]>(keybuf.data());
+    constexpr int SIZE = W::SIZE;
+    static_assert(SIZE % 16 == 0, "keys are hashed 16 at a time");
     uint8_t pk[2][64], blocks[2][64], h[2][16];
     for (int j = 0; j < 2; j++) {
         memcpy(pk[j] + 32, ed_pub, 32);
@@ -352,9 +627,10 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     uint32_t want[4], mask[4];
     lxmfv_prefix_words(s->prefix, s->nibbles, want, mask);
     while (!stopped(*s)) {
-        const uint64_t first = w.batch(keys, BATCH);
+        uint64_t first;
+        const uint8_t(*keys)[32] = w.next_group(&first);
         uint32_t hits16 = 0;
-        for (int i = 0; i < BATCH; i++) {
+        for (int i = 0; i < SIZE; i++) {
             // Keys are hashed sixteen at a time (AVX-512: a bit per matching
             // key) or in pairs (two SHA-256 streams interleaved where the CPU
             // has the SHA extensions), and checked in walk order.
@@ -386,7 +662,7 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
             s->tries.fetch_add((uint64_t)i + 1, std::memory_order_relaxed);
             return;
         }
-        s->tries.fetch_add(BATCH, std::memory_order_relaxed);
+        s->tries.fetch_add(SIZE, std::memory_order_relaxed);
     }
 }
 
@@ -404,6 +680,38 @@ bool use_x16() {
 #else
     return false;
 #endif
+}
+
+bool use_ifma() {
+#if defined(__x86_64__)
+    return ifma::available();
+#else
+    return false;
+#endif
+}
+
+// The walk: the IFMA lanes where the CPU has them; LXMFV_CPU_WALK=scalar|ifma
+// picks one (tests run each).  -1 where the choice is unknown or unavailable.
+int walk_kind() {
+    const char* force = getenv("LXMFV_CPU_WALK");
+    if (!force) return use_ifma() ? 1 : 0;
+    if (!strcmp(force, "scalar")) return 0;
+    if (!strcmp(force, "ifma") && use_ifma()) return 1;
+    return -1;
+}
+
+template <class W>
+int walk_keys(const uint8_t start[32], uint64_t count, uint8_t* keys) {
+    W w;
+    if (w.init(start) != LXMFV_OK) return LXMFV_ERR_STATE;
+    for (uint64_t done = 0; done < count;) {
+        uint64_t first;
+        const uint8_t(*g)[32] = w.next_group(&first);
+        const uint64_t len = std::min<uint64_t>(W::SIZE, count - done);
+        memcpy(keys + 32 * done, g, 32 * (size_t)len);
+        done += len;
+    }
+    return LXMFV_OK;
 }
 
 }  // namespace
@@ -453,16 +761,16 @@ extern "C" int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uin
 
 extern "C" int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys) {
     if (!start || (count && !keys)) return LXMFV_ERR_ARG;
-    Walk w;
-    if (w.init(start) != LXMFV_OK) return LXMFV_ERR_STATE;
-    std::vector<uint8_t> tmp(BATCH * 32);
-    for (uint64_t done = 0; done < count;) {
-        const int len = (int)std::min<uint64_t>(BATCH, count - done);
-        w.batch(reinterpret_cast<uint8_t(*)[32]>(tmp.data()), len);
-        memcpy(keys + 32 * done, tmp.data(), 32 * (size_t)len);
-        done += (uint64_t)len;
+    switch (walk_kind()) {
+        case 0:
+            return walk_keys<Walk>(start, count, keys);
+#if defined(__x86_64__)
+        case 1:
+            return walk_keys<WalkIfma>(start, count, keys);
+#endif
+        default:
+            return LXMFV_ERR_STATE;
     }
-    return LXMFV_OK;
 }
 
 extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
@@ -515,20 +823,31 @@ extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uin
     s.identity_out = identity;
     std::vector<std::thread> pool;
     pool.reserve((size_t)threads);
-    // The fastest hasher this CPU has; LXMFV_CPU_HASH=c|ni|x16 picks one (tests
-    // run each), LXMFV_ERR_STATE where the CPU lacks it.
-    void (*run)(Shared*, const uint8_t*, const uint8_t*) =
-        use_x16() ? walker<HASH_X16> : use_sha_ni() ? walker<HASH_NI> : walker<HASH_C>;
+    // The fastest walk and hasher this CPU has; LXMFV_CPU_WALK=scalar|ifma and
+    // LXMFV_CPU_HASH=c|ni|x16 pick one (tests run each), LXMFV_ERR_STATE where
+    // the CPU lacks it.
+    int hash = use_x16() ? HASH_X16 : use_sha_ni() ? HASH_NI : HASH_C;
     if (const char* force = getenv("LXMFV_CPU_HASH")) {
         if (!strcmp(force, "c"))
-            run = walker<HASH_C>;
+            hash = HASH_C;
         else if (!strcmp(force, "ni") && use_sha_ni())
-            run = walker<HASH_NI>;
+            hash = HASH_NI;
         else if (!strcmp(force, "x16") && use_x16())
-            run = walker<HASH_X16>;
+            hash = HASH_X16;
         else
             return LXMFV_ERR_STATE;
     }
+    const int walk = walk_kind();
+    if (walk < 0) return LXMFV_ERR_STATE;
+    void (*run)(Shared*, const uint8_t*, const uint8_t*) = nullptr;
+#if defined(__x86_64__)
+    if (walk == 1)
+        run = hash == HASH_X16 ? walker<HASH_X16, WalkIfma>
+              : hash == HASH_NI ? walker<HASH_NI, WalkIfma>
+                                : walker<HASH_C, WalkIfma>;
+#endif
+    if (!run)
+        run = hash == HASH_X16 ? walker<HASH_X16, Walk> : hash == HASH_NI ? walker<HASH_NI, Walk> : walker<HASH_C, Walk>;
     for (int t = 0; t < threads; t++) pool.emplace_back(run, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
     while (!stopped(s)) {
         if (tries) __atomic_store_n(tries, s.tries.load(std::memory_order_relaxed), __ATOMIC_RELAXED);

@@ -24,13 +24,38 @@ def config1():
         return json.load(f)
 
 
-def test_walk_matches_the_oracle(lx):
+def use_walk(lx, monkeypatch, walk):
+    """Select the CPU walk (scalar 5 x 51-bit, or the AVX-512 IFMA lanes);
+    skips where this CPU has no IFMA."""
+    monkeypatch.setenv("LXMFV_CPU_WALK", walk)
+    try:
+        lx.cpu_walk(bytes(lx.seeded_identity(1)[0][:32]), 1)
+    except lx.LxmfvError as e:
+        assert walk == "ifma" and e.code == lx.ERR_STATE
+        pytest.skip("this CPU has no AVX-512 IFMA")
+
+
+@pytest.mark.parametrize("walk", ["scalar", "ifma"])
+def test_walk_matches_the_oracle(lx, monkeypatch, walk):
+    """Both walks, across their group boundaries (256 keys scalar, 2048 on the
+    IFMA lanes)."""
+    use_walk(lx, monkeypatch, walk)
     for seed in (1, 2, 99):
         ident, _ = lx.seeded_identity(seed)
-        for count in (0, 1, 255, 256, 257, 1000):
+        for count in (0, 1, 255, 256, 257, 1000, 2047, 2048, 2049, 4500):
             got = lx.cpu_walk(ident[:32], count)
             assert got.shape == (count, 32)
             assert np.array_equal(got, O.walk_keys(ident[:32], count)), (seed, count)
+
+
+def test_unknown_walk_is_refused(lx, monkeypatch):
+    monkeypatch.setenv("LXMFV_CPU_WALK", "montgomery")
+    with pytest.raises(lx.LxmfvError) as e:
+        lx.cpu_walk(bytes(32), 1)
+    assert e.value.code == lx.ERR_STATE
+    with pytest.raises(lx.LxmfvError) as e:
+        lx.CpuSearch(lx.prefix_parse("c3"), threads=1, seed=13).run()
+    assert e.value.code == lx.ERR_STATE
 
 
 def test_walk_keys_are_x25519_of_the_stepped_scalars(lx):
@@ -99,12 +124,14 @@ def test_seeded_walker_matches_the_oracle(lx, walker):
     assert s.tries == int(hits[0]) + 1
 
 
+@pytest.mark.parametrize("walk", ["scalar", "ifma"])
 @pytest.mark.parametrize("hasher", ["c", "ni", "x16"])
 @pytest.mark.parametrize("prefix_text", ["c3", "e01"])
-def test_every_hasher_finds_the_first_hit(lx, monkeypatch, hasher, prefix_text):
-    """Each of the search's hashers (portable C, SHA extensions in pairs,
-    AVX-512 sixteen at a time) returns the oracle's first hit in walk order,
-    with the same tries."""
+def test_every_hasher_finds_the_first_hit(lx, monkeypatch, walk, hasher, prefix_text):
+    """Each walk with each of the search's hashers (portable C, SHA extensions
+    in pairs, AVX-512 sixteen at a time) returns the oracle's first hit in walk
+    order, with the same tries."""
+    use_walk(lx, monkeypatch, walk)
     monkeypatch.setenv("LXMFV_CPU_HASH", hasher)
     seed, prefix = 13, O.prefix_parse(prefix_text)
     k0, ed_seed, _ = O.seeded_identity(seed)
