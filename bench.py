@@ -87,7 +87,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
     p.add_argument("--no-b64", action="store_true", help="skip the second measurement at B = 64")
     p.add_argument("--no-batched", action="store_true", help="skip the 256-search batched measurement")
-    p.add_argument("--served-seconds", type=float, default=20.0,
+    p.add_argument("--served-seconds", type=float, default=60.0,
                    help="length of the served-requests run (0: skip); the full served workload is 600")
     return p.parse_args()
 
