@@ -596,13 +596,14 @@ inline void hash_pair(uint8_t pk[2][64], uint8_t blocks[2][64], uint8_t h[2][16]
     cpu_sha::address<false>(pk[1], blocks[1], h[1]);
 }
 
-// Bit m set where key first + m of `keys` (16 of them) matches the prefix.
-inline uint32_t match16(const uint8_t (*keys)[32], const uint8_t* ed_pub, const uint8_t* nh, const uint32_t want[4],
+// Bit m set where key m of `keys` (16 of them, sharing the ed_pub and name
+// hash folded into `shared`) matches the prefix.
+inline uint32_t match16(const uint8_t (*keys)[32], const cpu_sha::Shared16& shared, const uint32_t want[4],
                         const uint32_t mask[4]) {
 #if defined(__x86_64__)
-    return cpu_sha::x16::match16(keys[0], 32, ed_pub, nh, want, mask);
+    return cpu_sha::x16::match16_shared(keys[0], 32, shared, want, mask);
 #else
-    (void)keys, (void)ed_pub, (void)nh, (void)want, (void)mask;
+    (void)keys, (void)shared, (void)want, (void)mask;
     return 0;
 #endif
 }
@@ -626,6 +627,8 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     }
     uint32_t want[4], mask[4];
     lxmfv_prefix_words(s->prefix, s->nibbles, want, mask);
+    cpu_sha::Shared16 shared;
+    cpu_sha::shared16_init(ed_pub, s->nh, &shared);
     while (!stopped(*s)) {
         uint64_t first;
         const uint8_t(*keys)[32] = w.next_group(&first);
@@ -635,7 +638,7 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
             // key) or in pairs (two SHA-256 streams interleaved where the CPU
             // has the SHA extensions), and checked in walk order.
             if (H == HASH_X16) {
-                if ((i & 15) == 0) hits16 = match16(keys + i, ed_pub, s->nh, want, mask);
+                if ((i & 15) == 0) hits16 = match16(keys + i, shared, want, mask);
                 if (!(hits16 >> (i & 15) & 1)) {
                     if (!(hits16 >> (i & 15))) i |= 15;  // no match left in these 16
                     continue;
@@ -724,9 +727,25 @@ extern "C" int lxmfv_cpu_addresses(const uint8_t* pks, uint64_t count, const uin
     if (impl == 0 && use_x16()) impl = 4;
 #if defined(__x86_64__)
     if (impl == 4) {
+        // Sixteen keys with one ed_pub (a walker's keys) take the path that
+        // folds ed_pub and the name hash in once; others the general one.
         uint64_t i = 0;
-        for (; i + 16 <= count; i += 16)
-            cpu_sha::x16::address16_bytes(pks + 64 * i, 64, pks + 64 * i + 32, 64, name_hash, out + 16 * i);
+        cpu_sha::Shared16 shared;
+        const uint8_t* shared_ed = nullptr;
+        for (; i + 16 <= count; i += 16) {
+            const uint8_t* ed = pks + 64 * i + 32;
+            bool same = true;
+            for (int m = 1; m < 16 && same; m++) same = !memcmp(ed, ed + 64 * m, 32);
+            if (!same) {
+                cpu_sha::x16::address16_bytes(pks + 64 * i, 64, ed, 64, name_hash, out + 16 * i);
+                continue;
+            }
+            if (!shared_ed || memcmp(shared_ed, ed, 32)) {
+                cpu_sha::shared16_init(ed, name_hash, &shared);
+                shared_ed = ed;
+            }
+            cpu_sha::x16::address16_shared_bytes(pks + 64 * i, 64, shared, out + 16 * i);
+        }
         if (i < count) {
             // The last keys, padded to 16 with copies of the final one.
             uint8_t tail[16][64], addrs[16][16];

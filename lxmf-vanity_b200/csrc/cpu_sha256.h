@@ -256,6 +256,65 @@ struct PadKW {
 };
 constexpr PadKW PAD_KW{};
 
+// ---- Sixteen keys that share one ed_pub and one name hash (a walker's keys).
+// Block 1's words 8..15 (ed_pub) and block 3's words 0, 1 (name hash) and
+// 7..15 (zeros, length) are the same for every key, so what depends on them
+// alone is computed once, in scalar code: block 1's first round, the K + W of
+// its rounds 8..15 and the constant parts of its schedule words 16..31; block
+// 3's first two rounds and the constant parts of its words 16..31.
+
+inline uint32_t s_ssig0(uint32_t x) { return rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3); }
+inline uint32_t s_ssig1(uint32_t x) { return rotr(x, 17) ^ rotr(x, 19) ^ (x >> 10); }
+
+struct Shared16 {
+    uint32_t t1c, t2c;  // block 1, round 0: T1 = t1c + W0, T2 = t2c
+    uint32_t kw1[8];    // block 1: K[8 + i] + W[8 + i]
+    uint32_t c1[16];    // block 1: the ed_pub-only part of W[16 + i]
+    uint32_t s3[8];     // block 3: the state after rounds 0 and 1
+    uint32_t nh2;       // block 3: W2's name-hash half
+    uint32_t c3_16, c3_17, c3_18, c3_30, c3_31;
+};
+
+inline void shared16_init(const uint8_t ed[32], const uint8_t nh[10], Shared16* c) {
+    uint32_t e[8];
+    for (int i = 0; i < 8; i++)
+        e[i] = (uint32_t)ed[4 * i] << 24 | (uint32_t)ed[4 * i + 1] << 16 | (uint32_t)ed[4 * i + 2] << 8 | ed[4 * i + 3];
+    auto bsig0 = [](uint32_t a) { return rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22); };
+    auto bsig1 = [](uint32_t x) { return rotr(x, 6) ^ rotr(x, 11) ^ rotr(x, 25); };
+    auto ch = [](uint32_t x, uint32_t y, uint32_t z) { return (x & y) ^ (~x & z); };
+    auto maj = [](uint32_t x, uint32_t y, uint32_t z) { return (x & y) ^ (x & z) ^ (y & z); };
+    c->t1c = IV[7] + bsig1(IV[4]) + ch(IV[4], IV[5], IV[6]) + K[0];
+    c->t2c = bsig0(IV[0]) + maj(IV[0], IV[1], IV[2]);
+    for (int i = 0; i < 8; i++) c->kw1[i] = K[8 + i] + e[i];
+    // W16 = s1(W14) + W9 + s0(W1) + W0, ...: the terms in W8..W15 = e0..e7.
+    c->c1[0] = s_ssig1(e[6]) + e[1];
+    c->c1[1] = s_ssig1(e[7]) + e[2];
+    for (int i = 2; i < 7; i++) c->c1[i] = e[i + 1];  // W18..W22: W11..W15
+    c->c1[7] = s_ssig0(e[0]);                         // W23: s0(W8)
+    for (int i = 8; i < 15; i++) c->c1[i] = s_ssig0(e[i - 7]) + e[i - 8];  // W24..W30: s0(W9..W15) + W8..W14
+    c->c1[15] = e[7];                                                       // W31: W15
+    // Block 3: name_hash[0..9] || identity hash || 0x80 || zeros || 208.
+    const uint32_t n0 = (uint32_t)nh[0] << 24 | (uint32_t)nh[1] << 16 | (uint32_t)nh[2] << 8 | nh[3];
+    const uint32_t n1 = (uint32_t)nh[4] << 24 | (uint32_t)nh[5] << 16 | (uint32_t)nh[6] << 8 | nh[7];
+    c->nh2 = (uint32_t)nh[8] << 24 | (uint32_t)nh[9] << 16;
+    uint32_t s[8];
+    memcpy(s, IV, sizeof s);
+    const uint32_t w01[2] = {n0, n1};
+    for (int r = 0; r < 2; r++) {
+        const uint32_t t1 = s[7] + bsig1(s[4]) + ch(s[4], s[5], s[6]) + K[r] + w01[r];
+        const uint32_t t2 = bsig0(s[0]) + maj(s[0], s[1], s[2]);
+        memmove(s + 1, s, 7 * sizeof(uint32_t));
+        s[4] += t1;
+        s[0] = t1 + t2;
+    }
+    memcpy(c->s3, s, sizeof s);
+    c->c3_16 = s_ssig0(n1) + n0;
+    c->c3_17 = s_ssig1(208) + n1;
+    c->c3_18 = s_ssig1(c->c3_16);
+    c->c3_30 = s_ssig0(208);
+    c->c3_31 = s_ssig0(c->c3_16) + 208;
+}
+
 #if defined(__x86_64__)
 // Sixteen addresses at once with AVX-512F: message m in 32-bit lane m of each
 // vector.  A rotate is one vprord, and Sigma0 / Sigma1 / sigma0 / sigma1's
@@ -290,7 +349,7 @@ LXCPU_X16 inline V bswap(V x) {
     }
 
 // One compression of the 16-word blocks w (schedule extended in place).
-LXCPU_X16 inline void compress(V s[8], V w[16]) {
+LXCPU_X16 __attribute__((always_inline)) inline void compress(V s[8], V w[16]) {
     V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
 #pragma GCC unroll 8
     for (int r = 0; r < 64; r += 8) {
@@ -322,7 +381,7 @@ LXCPU_X16 inline void compress(V s[8], V w[16]) {
 }
 
 // The padding block's compression: its K + W are the constants PAD_KW.
-LXCPU_X16 inline void compress_pad64(V s[8]) {
+LXCPU_X16 __attribute__((always_inline)) inline void compress_pad64(V s[8]) {
     V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], h = s[7];
 #pragma GCC unroll 8
     for (int r = 0; r < 64; r += 8) {
@@ -407,6 +466,167 @@ LXCPU_X16 inline uint32_t match16(const uint8_t* x, int x_stride, const uint8_t*
                                   const uint32_t want[4], const uint32_t mask[4]) {
     V h[4];
     address16(x, x_stride, ed, 0, nh, h);
+    __mmask16 m = 0xFFFF;
+    for (int i = 0; i < 4; i++)
+        if (mask[i])
+            m &= _mm512_cmpeq_epi32_mask(_mm512_and_si512(h[i], _mm512_set1_epi32((int)mask[i])),
+                                         _mm512_set1_epi32((int)want[i]));
+    return m;
+}
+
+#define LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, kw)                 \
+    {                                                              \
+        const V t1_ = add(add(h, kw), add(bsig1(e), ch(e, f, g))); \
+        d = add(d, t1_);                                           \
+        h = add(t1_, add(bsig0(a), maj(a, b, c)));                 \
+    }
+#define LXCPU_X16_K(r) _mm512_set1_epi32((int)K[r])
+#define LXCPU_X16_C(x) _mm512_set1_epi32((int)(x))
+
+// Rounds 16..63 with w[i & 15] = W_i for i = 16..31; the names are those of
+// round 16 (the caller's state after round 15).
+LXCPU_X16 __attribute__((always_inline)) inline void rounds_16_63(V& a, V& b, V& c, V& d, V& e, V& f, V& g, V& h, V w[16]) {
+#pragma GCC unroll 6
+    for (int r = 16; r < 64; r += 8) {
+        if (r >= 32) {
+#pragma GCC unroll 8
+            for (int j = 0; j < 8; j++) {
+                const int i = (r + j) & 15;
+                w[i] = add(add(w[i], ssig0(w[(i + 1) & 15])), add(w[(i + 9) & 15], ssig1(w[(i + 14) & 15])));
+            }
+        }
+        const int q = r & 15;
+        LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, add(w[q + 0], LXCPU_X16_K(r + 0)));
+        LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, add(w[q + 1], LXCPU_X16_K(r + 1)));
+        LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, add(w[q + 2], LXCPU_X16_K(r + 2)));
+        LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, add(w[q + 3], LXCPU_X16_K(r + 3)));
+        LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, add(w[q + 4], LXCPU_X16_K(r + 4)));
+        LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, add(w[q + 5], LXCPU_X16_K(r + 5)));
+        LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, add(w[q + 6], LXCPU_X16_K(r + 6)));
+        LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, add(w[q + 7], LXCPU_X16_K(r + 7)));
+    }
+}
+
+// Block 1 (x_pub words x[0..7], the shared ed_pub in c) from the initial state:
+// s = IV + the compression.
+LXCPU_X16 __attribute__((always_inline)) inline void block1_shared(const V x[8], const Shared16& k, V s[8]) {
+    // Round 0 on the constant initial state; the names are then round 1's.
+    const V t1 = add(x[0], LXCPU_X16_C(k.t1c));
+    V h = add(t1, LXCPU_X16_C(k.t2c)), d = add(t1, LXCPU_X16_C(IV[3]));
+    V a = LXCPU_X16_C(IV[0]), b = LXCPU_X16_C(IV[1]), c = LXCPU_X16_C(IV[2]);
+    V e = LXCPU_X16_C(IV[4]), f = LXCPU_X16_C(IV[5]), g = LXCPU_X16_C(IV[6]);
+    LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, add(x[1], LXCPU_X16_K(1)));
+    LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, add(x[2], LXCPU_X16_K(2)));
+    LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, add(x[3], LXCPU_X16_K(3)));
+    LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, add(x[4], LXCPU_X16_K(4)));
+    LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, add(x[5], LXCPU_X16_K(5)));
+    LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, add(x[6], LXCPU_X16_K(6)));
+    LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, add(x[7], LXCPU_X16_K(7)));
+    LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, LXCPU_X16_C(k.kw1[0]));
+    LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, LXCPU_X16_C(k.kw1[1]));
+    LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, LXCPU_X16_C(k.kw1[2]));
+    LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, LXCPU_X16_C(k.kw1[3]));
+    LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, LXCPU_X16_C(k.kw1[4]));
+    LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, LXCPU_X16_C(k.kw1[5]));
+    LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, LXCPU_X16_C(k.kw1[6]));
+    LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, LXCPU_X16_C(k.kw1[7]));
+    // W16..W31: x-dependent terms plus the constant parts.
+    V w[16];
+    w[0] = add(add(LXCPU_X16_C(k.c1[0]), ssig0(x[1])), x[0]);
+    w[1] = add(add(LXCPU_X16_C(k.c1[1]), ssig0(x[2])), x[1]);
+    for (int i = 2; i < 7; i++)
+        w[i] = add(add(LXCPU_X16_C(k.c1[i]), ssig1(w[i - 2])), add(ssig0(x[i + 1]), x[i]));
+    w[7] = add(add(LXCPU_X16_C(k.c1[7]), ssig1(w[5])), add(w[0], x[7]));
+    for (int i = 8; i < 15; i++) w[i] = add(add(LXCPU_X16_C(k.c1[i]), ssig1(w[i - 2])), w[i - 7]);
+    w[15] = add(add(LXCPU_X16_C(k.c1[15]), ssig1(w[13])), add(w[8], ssig0(w[0])));
+    rounds_16_63(a, b, c, d, e, f, g, h, w);
+    s[0] = add(a, LXCPU_X16_C(IV[0]));
+    s[1] = add(b, LXCPU_X16_C(IV[1]));
+    s[2] = add(c, LXCPU_X16_C(IV[2]));
+    s[3] = add(d, LXCPU_X16_C(IV[3]));
+    s[4] = add(e, LXCPU_X16_C(IV[4]));
+    s[5] = add(f, LXCPU_X16_C(IV[5]));
+    s[6] = add(g, LXCPU_X16_C(IV[6]));
+    s[7] = add(h, LXCPU_X16_C(IV[7]));
+}
+
+// Block 3 from the identity hash words ih[0..3]: the first four words of the
+// destination hash.
+LXCPU_X16 __attribute__((always_inline)) inline void block3_shared(const V ih[4], const Shared16& k, V out[4]) {
+    const V y2 = _mm512_or_si512(LXCPU_X16_C(k.nh2), _mm512_srli_epi32(ih[0], 16));
+    const V y3 = _mm512_or_si512(_mm512_slli_epi32(ih[0], 16), _mm512_srli_epi32(ih[1], 16));
+    const V y4 = _mm512_or_si512(_mm512_slli_epi32(ih[1], 16), _mm512_srli_epi32(ih[2], 16));
+    const V y5 = _mm512_or_si512(_mm512_slli_epi32(ih[2], 16), _mm512_srli_epi32(ih[3], 16));
+    const V y6 = _mm512_or_si512(_mm512_slli_epi32(ih[3], 16), LXCPU_X16_C(0x8000));
+    // The state after rounds 0 and 1, under round 2's names.
+    V g = LXCPU_X16_C(k.s3[0]), h = LXCPU_X16_C(k.s3[1]), a = LXCPU_X16_C(k.s3[2]), b = LXCPU_X16_C(k.s3[3]);
+    V c = LXCPU_X16_C(k.s3[4]), d = LXCPU_X16_C(k.s3[5]), e = LXCPU_X16_C(k.s3[6]), f = LXCPU_X16_C(k.s3[7]);
+    LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, add(y2, LXCPU_X16_K(2)));
+    LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, add(y3, LXCPU_X16_K(3)));
+    LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, add(y4, LXCPU_X16_K(4)));
+    LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, add(y5, LXCPU_X16_K(5)));
+    LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, add(y6, LXCPU_X16_K(6)));
+    LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, LXCPU_X16_K(7));  // W7..W14 = 0
+    LXCPU_X16_ROUND(a, b, c, d, e, f, g, h, LXCPU_X16_K(8));
+    LXCPU_X16_ROUND(h, a, b, c, d, e, f, g, LXCPU_X16_K(9));
+    LXCPU_X16_ROUND(g, h, a, b, c, d, e, f, LXCPU_X16_K(10));
+    LXCPU_X16_ROUND(f, g, h, a, b, c, d, e, LXCPU_X16_K(11));
+    LXCPU_X16_ROUND(e, f, g, h, a, b, c, d, LXCPU_X16_K(12));
+    LXCPU_X16_ROUND(d, e, f, g, h, a, b, c, LXCPU_X16_K(13));
+    LXCPU_X16_ROUND(c, d, e, f, g, h, a, b, LXCPU_X16_K(14));
+    LXCPU_X16_ROUND(b, c, d, e, f, g, h, a, LXCPU_X16_C(K[15] + 208u));  // W15 = 208
+    V w[16];
+    w[0] = LXCPU_X16_C(k.c3_16);
+    w[1] = add(LXCPU_X16_C(k.c3_17), ssig0(y2));
+    w[2] = add(add(LXCPU_X16_C(k.c3_18), ssig0(y3)), y2);
+    w[3] = add(add(ssig1(w[1]), ssig0(y4)), y3);
+    w[4] = add(add(ssig1(w[2]), ssig0(y5)), y4);
+    w[5] = add(add(ssig1(w[3]), ssig0(y6)), y5);
+    w[6] = add(add(ssig1(w[4]), LXCPU_X16_C(208)), y6);
+    w[7] = add(ssig1(w[5]), w[0]);
+    for (int i = 8; i < 14; i++) w[i] = add(ssig1(w[i - 2]), w[i - 7]);
+    w[14] = add(add(ssig1(w[12]), w[7]), LXCPU_X16_C(k.c3_30));
+    w[15] = add(add(ssig1(w[13]), w[8]), LXCPU_X16_C(k.c3_31));
+    rounds_16_63(a, b, c, d, e, f, g, h, w);
+    out[0] = add(a, LXCPU_X16_C(IV[0]));
+    out[1] = add(b, LXCPU_X16_C(IV[1]));
+    out[2] = add(c, LXCPU_X16_C(IV[2]));
+    out[3] = add(d, LXCPU_X16_C(IV[3]));
+}
+#undef LXCPU_X16_ROUND
+#undef LXCPU_X16_K
+#undef LXCPU_X16_C
+
+// address16 for 16 keys that share the ed_pub and name hash in k.
+LXCPU_X16 inline void address16_shared(const uint8_t* x, int x_stride, const Shared16& k, V out[4]) {
+    const V lane = _mm512_set_epi32(15, 14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0);
+    const V xoff = _mm512_mullo_epi32(lane, _mm512_set1_epi32(x_stride));
+    V xw[8], s[8];
+    for (int j = 0; j < 8; j++) xw[j] = bswap(_mm512_i32gather_epi32(xoff, (const void*)(x + 4 * j), 1));
+    block1_shared(xw, k, s);
+    compress_pad64(s);
+    block3_shared(s, k, out);
+}
+
+LXCPU_X16 inline void address16_shared_bytes(const uint8_t* x, int x_stride, const Shared16& k, uint8_t* out) {
+    V h[4];
+    address16_shared(x, x_stride, k, h);
+    alignas(64) uint32_t words[4][16];
+    for (int i = 0; i < 4; i++) _mm512_store_si512((void*)words[i], h[i]);
+    for (int m = 0; m < 16; m++)
+        for (int i = 0; i < 4; i++) {
+            out[16 * m + 4 * i] = (uint8_t)(words[i][m] >> 24);
+            out[16 * m + 4 * i + 1] = (uint8_t)(words[i][m] >> 16);
+            out[16 * m + 4 * i + 2] = (uint8_t)(words[i][m] >> 8);
+            out[16 * m + 4 * i + 3] = (uint8_t)words[i][m];
+        }
+}
+
+// match16 for keys sharing the ed_pub and name hash in k.
+LXCPU_X16 inline uint32_t match16_shared(const uint8_t* x, int x_stride, const Shared16& k, const uint32_t want[4],
+                                         const uint32_t mask[4]) {
+    V h[4];
+    address16_shared(x, x_stride, k, h);
     __mmask16 m = 0xFFFF;
     for (int i = 0; i < 4; i++)
         if (mask[i])
