@@ -382,20 +382,27 @@ LXCPU_IFMA inline FV carry(FV a) {
     return a;
 }
 
-LXCPU_IFMA inline FV add(const FV& a, const FV& b) {
+// a + b without the carry: limbs up to 2^52 + 2^51, fit only for sub's b.
+LXCPU_IFMA inline FV add_loose(const FV& a, const FV& b) {
     FV r;
     for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(a.l[k], b.l[k]);
-    return carry(r);
+    return r;
 }
 
-// a - b + 4p, as the scalar sub.
-LXCPU_IFMA inline FV sub(const FV& a, const FV& b) {
+LXCPU_IFMA inline FV add(const FV& a, const FV& b) { return carry(add_loose(a, b)); }
+
+// a - b + 4p without the carry (b's limbs at most 4p's, about 2^53): limbs
+// below 2^54, fit only for to_words (which carries first) or carry().
+LXCPU_IFMA inline FV sub_loose(const FV& a, const FV& b) {
     FV r;
     r.l[0] = _mm512_sub_epi64(_mm512_add_epi64(a.l[0], _mm512_set1_epi64((long long)(4 * (MASK51 - 18)))), b.l[0]);
     for (int k = 1; k < 5; k++)
         r.l[k] = _mm512_sub_epi64(_mm512_add_epi64(a.l[k], _mm512_set1_epi64((long long)(4 * MASK51))), b.l[k]);
-    return carry(r);
+    return r;
 }
+
+// a - b + 4p, as the scalar sub.
+LXCPU_IFMA inline FV sub(const FV& a, const FV& b) { return carry(sub_loose(a, b)); }
 
 // a * b mod p.  A 52 x 52-bit product splits at bit 52: its low half goes to
 // column i + j and its high half, worth 2^52 = 2 * 2^51, to column i + j + 1
@@ -438,7 +445,9 @@ LXCPU_IFMA inline FV sqr(const FV& a) {
 }
 
 // The canonical encodings of the eight lanes as four little-endian 64-bit
-// words each (w[i] lane j), as the scalar to_bytes.
+// words each (w[i] lane j), as the scalar to_bytes.  Limbs below 2^63 in: one
+// carry leaves a value below 2^255 + 2^52 < 2p, where q = [a >= p] is the
+// carry out of a + 19.
 LXCPU_IFMA inline void to_words(FV a, V w[4]) {
     a = carry(a);
     const V m = _mm512_set1_epi64((long long)MASK51);
@@ -509,7 +518,7 @@ LXCPU_IFMA void group(F& uc, F& vc, Scratch* s) {
         const FV TU = load(t.u[r]), TV = load(t.v[r]);
         const FV invi = mul(INV, load(s->pre[r]));  // 1 / (u_{T_i} - u_C)
         INV = mul(INV, sub(TU, UC));
-        const FV sum = add(S0, TU);
+        const FV sum = add_loose(S0, TU);  // only ever subtracted
         const FV lp = mul(sub(TV, VC), invi);
         const FV lm = mul(add(TV, VC), invi);
         int rows_m[8], rows_p[8];
@@ -518,8 +527,8 @@ LXCPU_IFMA void group(F& uc, F& vc, Scratch* s) {
             rows_m[j] = M - i;                  // C - T_i: key c - i
             rows_p[j] = i < M ? M + i : -1;     // C + T_i: key c + i (C + T_M starts the next group)
         }
-        store_keys(sub(sqr(lm), sum), s->buf, rows_m);
-        store_keys(sub(sqr(lp), sum), s->buf, rows_p);
+        store_keys(sub_loose(sqr(lm), sum), s->buf, rows_m);  // to_words carries
+        store_keys(sub_loose(sqr(lp), sum), s->buf, rows_p);
     }
     // T_0 = J: the centre's own key, and the next centre C + J.
     to_bytes(s->buf[M], uc);
