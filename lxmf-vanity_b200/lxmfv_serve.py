@@ -235,6 +235,7 @@ class Request:
     tries: int | None = None   # keys before and including the hit, in walk order
     walked: int | None = None  # keys the search had walked when its hit was reported
     hit: tuple[int, int] | None = None  # (lane, n)
+    failed: bool = False  # its hit failed the recheck: no identity is returned
 
 
 def lanes_by_difficulty(nibbles: int, base: int = 64, cap: int = 32768) -> int:
@@ -273,11 +274,16 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
     """Runs the request loop until every request is done (or time_limit).
     Each step: admit arrived requests while the pool has lanes (continuous
     batching), walk every admitted search one step, retire searches on their
-    first hit (the hit with the smallest (n, lane), rechecked from scratch)."""
+    first hit (the hit with the smallest (n, lane), rechecked from scratch).
+    A hit that fails its recheck fails its request (the reference stops with
+    an error, main.rs:310-313): the search is retired without an identity and
+    counted in `rechecked_bad`; the other requests go on.  A request that an
+    empty pool refuses (larger than its memory budget) fails at once."""
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     waiting: deque[Request] = deque()
     active: dict[int, Request] = {}
     done: list[Request] = []
+    failed: list[Request] = []
     t0 = time.perf_counter()
     steps = 0
     keys = 0
@@ -293,9 +299,16 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
             try:
                 sid = pool.submit(waiting[0].spec)
             except lx.LxmfvError as e:
-                if e.code == lx.ERR_OVERFLOW:
+                if e.code != lx.ERR_OVERFLOW:
+                    raise
+                if active:
                     break  # no lanes free: it waits for a retirement
-                raise
+                # Refused by an empty pool: larger than the whole memory budget.
+                r = waiting.popleft()
+                r.failed = True
+                r.done = time.perf_counter() - t0
+                failed.append(r)
+                continue
             r = waiting.popleft()
             r.admitted = time.perf_counter() - t0
             active[sid] = r
@@ -318,6 +331,11 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
             r = active.pop(sid)
             if not r.spec.recheck(lane, n):
                 bad += 1
+                r.failed = True
+                r.done = t_now
+                pool.retire(sid)
+                failed.append(r)
+                continue
             r.done = t_now
             r.hit = (lane, n)
             # Lanes advance in step: the hit is key number n * lanes + lane + 1 in walk order.
@@ -326,11 +344,11 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
             pool.retire(sid)
             done.append(r)
     wall = time.perf_counter() - t0
-    return summarise(done, requests, wall, keys, busy_ms, steps, bad)
+    return summarise(done, requests, wall, keys, busy_ms, steps, bad, failed=len(failed))
 
 
 def summarise(done: list[Request], requests: list[Request], wall: float, keys: int, busy_ms: float, steps: int,
-              bad: int) -> dict:
+              bad: int, failed: int = 0) -> dict:
     norm_tries = np.array([r.tries / expected_tries(r.spec.nibbles) for r in done]) if done else np.zeros(0)
     # Time in service at the search's own (constant, per step) key rate is its
     # walked keys over that rate, so its time over the expected time is the
@@ -341,7 +359,7 @@ def summarise(done: list[Request], requests: list[Request], wall: float, keys: i
     q = lambda a, p: float(np.quantile(a, p)) if len(a) else float("nan")  # noqa: E731
     targets = {"p50": math.log(2), "p95": math.log(20), "p99": math.log(100)}
     out = {
-        "requests": len(requests), "done": len(done), "wall_s": wall, "steps": steps,
+        "requests": len(requests), "done": len(done), "failed": failed, "wall_s": wall, "steps": steps,
         "aggregate_keys_per_s": rate, "busy_fraction": busy_ms * 1e-3 / wall if wall > 0 else 0.0,
         "rechecked_bad": bad,
         "tries_over_expected": {k: q(norm_tries, p) for k, p in (("p50", .5), ("p95", .95), ("p99", .99))},
