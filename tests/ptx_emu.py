@@ -4,8 +4,9 @@ be checked against Python integers on a machine without a GPU.
 
 Only what the blocks use is implemented: mul/mad/madc (.lo/.hi, with and
 without .cc), add/addc, sub/subc (.cc), shf.l.wrap, shl, shr (.u32/.s32),
-and, xor, mov, setp.eq.u32, and a predicated (@p / @!p) bra to a label of
-the same block.  CC.CF is the carry (or the borrow, for sub/subc) flag.
+and, xor, mov, setp (eq, ne, lt, le, gt, ge on .u32), and a predicated
+(@p / @!p) bra to a label of the same block.  CC.CF is the carry (or the
+borrow, for sub/subc) flag.
 """
 from __future__ import annotations
 
@@ -96,12 +97,15 @@ def run(lines: list[str], args: list[int], branches: dict | None = None) -> list
             continue
         if guard is not None:
             raise NotImplementedError("predicated " + op)
-        if op == "setp.eq.u32":
-            preds[ops[0]] = val(ops[1]) == val(ops[2])
-            continue
         parts = op.split(".")
         base = parts[0]
         mods = set(parts[1:])
+        if base == "setp":
+            x, y = val(ops[1]), val(ops[2])
+            assert "u32" in mods, op
+            cmp = {"eq": x == y, "ne": x != y, "lt": x < y, "le": x <= y, "gt": x > y, "ge": x >= y}
+            preds[ops[0]] = next(v for k, v in cmp.items() if k in mods)
+            continue
         cc = "cc" in mods
         d = ops[0]
         if base in ("mul", "mad", "madc"):
