@@ -333,15 +333,16 @@ def main() -> None:
                       a.warmup, e2e=False)
         line["at_batch_64"] = {"value": b64["value"], "unit": "keys/s", "ms_per_step": b64["ms_per_step"],
                                "config": b64["config"], "clocks": b64["clocks"], "hits": b64["hits"]}
+    # The side sections run once, on a single-GPU run (rank 0 of world 1).
     if rank == 0 and world == 1 and not a.no_batched:
         line["batched"] = batched_workload(lx, dev, head["value"])
     if rank == 0 and world == 1 and a.served_seconds > 0:
         line["served"] = served_workload(dev, a.served_seconds)
-    if rank == 0 and not a.no_cpu_baseline:
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prefix)
-    if rank == 0 and not a.no_cpu_search:
+    if rank == 0 and world == 1 and not a.no_cpu_search:
         line["cpu_search"] = cpu_search_rate()
-    if rank == 0 and not a.no_ref_cuda:
+    if rank == 0 and world == 1 and not a.no_ref_cuda:
         with lx.Backend(device=dev, lanes=1024) as b:
             line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)
     if world > 1:
