@@ -295,12 +295,24 @@ struct Walk {
         vc = vnext;
     }
 
-    // The next group's SIZE keys in walk order; *first: the walk index of the first.
-    const uint8_t (*next_group(uint64_t* first))[32] {
+    // The next group; *first: the walk index of its first key.
+    void advance(uint64_t* first) {
         group();
         *first = next;
         next += SIZE;
-        return buf;
+    }
+
+    // The group's keys as 32-byte rows in walk order.
+    const uint8_t (*keys())[32] { return buf; }
+
+    // Bit m set where key i + m of the group matches (i a multiple of 16).
+    uint32_t match16(int i, const cpu_sha::Shared16& shared, const uint32_t want[4], const uint32_t mask[4]) const {
+#if defined(__x86_64__)
+        return cpu_sha::x16::match16_shared(buf[i], 32, shared, want, mask);
+#else
+        (void)i, (void)shared, (void)want, (void)mask;
+        return 0;
+#endif
     }
 };
 
@@ -465,25 +477,37 @@ LXCPU_IFMA inline void to_words(FV a, V w[4]) {
     w[3] = _mm512_or_si512(_mm512_srli_epi64(a.l[3], 39), _mm512_slli_epi64(a.l[4], 12));
 }
 
-// Lane j's encoding into out[rows[j]].
-LXCPU_IFMA inline void store_keys(const FV& a, uint8_t (*out)[32], const int rows[8]) {
+// Keys are stored word-major: words[j][k] is 32-bit word j (little-endian)
+// of key k of the group, so that sixteen keys' word j is one vector load for
+// the hasher.  STRIDE leaves room past the last key for a full store.
+constexpr int STRIDE = 2 * M + 16;
+
+// The eight lanes' encodings into keys base .. base + 7 of words (lane j to
+// key base + j, or to base + 7 - j when `reverse`).
+LXCPU_IFMA inline void store_words(const FV& a, uint32_t (*words)[STRIDE], int base, bool reverse) {
     V w[4];
     to_words(a, w);
-    alignas(64) uint64_t t[4][8];
-    for (int i = 0; i < 4; i++) _mm512_store_si512((void*)t[i], w[i]);
-    for (int j = 0; j < 8; j++) {
-        if (rows[j] < 0) continue;
-        for (int i = 0; i < 4; i++) memcpy(out[rows[j]] + 8 * i, &t[i][j], 8);
+    const __m256i rev = _mm256_set_epi32(0, 1, 2, 3, 4, 5, 6, 7);
+    for (int i = 0; i < 4; i++) {
+        __m256i lo = _mm512_cvtepi64_epi32(w[i]);
+        __m256i hi = _mm512_cvtepi64_epi32(_mm512_srli_epi64(w[i], 32));
+        if (reverse) {
+            lo = _mm256_permutevar8x32_epi32(lo, rev);
+            hi = _mm256_permutevar8x32_epi32(hi, rev);
+        }
+        _mm256_storeu_si256((__m256i*)(words[2 * i] + base), lo);
+        _mm256_storeu_si256((__m256i*)(words[2 * i + 1] + base), hi);
     }
 }
 
 struct Scratch {
     Lanes pre[ROWS];  // lane j, row r: the product of its elements before row r
     Lanes acc;
-    uint8_t buf[2 * M][32];
+    alignas(64) uint32_t words[8][STRIDE];
+    uint8_t buf[2 * M][32];  // the same keys as bytes, filled on request
 };
 
-// One group: scratch->buf gets keys c - M .. c + M - 1 in walk order, and
+// One group: scratch->words gets keys c - M .. c + M - 1 in walk order, and
 // (uc, vc) moves to the next centre C + J.  The denominators u_{T_i} - u_C,
 // i = 1..M, are eight interleaved Montgomery chains (one per lane); their
 // eight totals and T_0's denominator share one scalar inversion.
@@ -521,17 +545,17 @@ LXCPU_IFMA void group(F& uc, F& vc, Scratch* s) {
         const FV sum = add_loose(S0, TU);  // only ever subtracted
         const FV lp = mul(sub(TV, VC), invi);
         const FV lm = mul(add(TV, VC), invi);
-        int rows_m[8], rows_p[8];
-        for (int j = 0; j < 8; j++) {
-            const int i = 1 + j + 8 * r;
-            rows_m[j] = M - i;                  // C - T_i: key c - i
-            rows_p[j] = i < M ? M + i : -1;     // C + T_i: key c + i (C + T_M starts the next group)
-        }
-        store_keys(sub_loose(sqr(lm), sum), s->buf, rows_m);  // to_words carries
-        store_keys(sub_loose(sqr(lp), sum), s->buf, rows_p);
+        // Lane j holds i = 1 + j + 8r: C - T_i is key M - i (rows M - 8 - 8r ..
+        // M - 1 - 8r, lanes reversed), C + T_i key M + i (rows M + 1 + 8r ..
+        // M + 8 + 8r; the last block's lane 7, C + T_M, starts the next group
+        // and lands in the slack past key 2M - 1).
+        store_words(sub_loose(sqr(lm), sum), s->words, M - 8 - 8 * r, true);  // to_words carries
+        store_words(sub_loose(sqr(lp), sum), s->words, M + 1 + 8 * r, false);
     }
     // T_0 = J: the centre's own key, and the next centre C + J.
-    to_bytes(s->buf[M], uc);
+    uint8_t centre[32];
+    to_bytes(centre, uc);
+    for (int j = 0; j < 8; j++) memcpy(&s->words[j][M], centre + 4 * j, 4);
     const F lp = ::mul(::sub(t.v0, vc), inv_d0);
     const F up = ::sub(::sqr(lp), ::add(s0, t.u0));
     vc = ::sub(::mul(lp, ::sub(uc, up)), vc);
@@ -564,11 +588,23 @@ struct WalkIfma {
         return LXMFV_OK;
     }
 
-    const uint8_t (*next_group(uint64_t* first))[32] {
+    // The next group; *first: the walk index of its first key.
+    void advance(uint64_t* first) {
         ifma::group(uc, vc, s.get());
         *first = next;
         next += SIZE;
+    }
+
+    // The group's keys as 32-byte rows in walk order.
+    const uint8_t (*keys())[32] {
+        for (int k = 0; k < SIZE; k++)
+            for (int j = 0; j < 8; j++) memcpy(s->buf[k] + 4 * j, &s->words[j][k], 4);
         return s->buf;
+    }
+
+    // Bit m set where key i + m of the group matches (i a multiple of 16).
+    uint32_t match16(int i, const cpu_sha::Shared16& shared, const uint32_t want[4], const uint32_t mask[4]) const {
+        return cpu_sha::x16::match16_shared_words(&s->words[0][i], ifma::STRIDE, shared, want, mask);
     }
 };
 #endif
@@ -605,18 +641,6 @@ inline void hash_pair(uint8_t pk[2][64], uint8_t blocks[2][64], uint8_t h[2][16]
     cpu_sha::address<false>(pk[1], blocks[1], h[1]);
 }
 
-// Bit m set where key m of `keys` (16 of them, sharing the ed_pub and name
-// hash folded into `shared`) matches the prefix.
-inline uint32_t match16(const uint8_t (*keys)[32], const cpu_sha::Shared16& shared, const uint32_t want[4],
-                        const uint32_t mask[4]) {
-#if defined(__x86_64__)
-    return cpu_sha::x16::match16_shared(keys[0], 32, shared, want, mask);
-#else
-    (void)keys, (void)shared, (void)want, (void)mask;
-    return 0;
-#endif
-}
-
 // One walker: search (main.rs:292-323) from scalar `start` with Ed25519 seed
 // `ed_seed`, walking with W (Walk, or WalkIfma on the IFMA lanes).
 template <Hasher H, class W>
@@ -640,14 +664,15 @@ void walker(Shared* s, const uint8_t* start, const uint8_t* ed_seed) {
     cpu_sha::shared16_init(ed_pub, s->nh, &shared);
     while (!stopped(*s)) {
         uint64_t first;
-        const uint8_t(*keys)[32] = w.next_group(&first);
+        w.advance(&first);
+        const uint8_t(*keys)[32] = H == HASH_X16 ? nullptr : w.keys();
         uint32_t hits16 = 0;
         for (int i = 0; i < SIZE; i++) {
             // Keys are hashed sixteen at a time (AVX-512: a bit per matching
             // key) or in pairs (two SHA-256 streams interleaved where the CPU
             // has the SHA extensions), and checked in walk order.
             if (H == HASH_X16) {
-                if ((i & 15) == 0) hits16 = match16(keys + i, shared, want, mask);
+                if ((i & 15) == 0) hits16 = w.match16(i, shared, want, mask);
                 if (!(hits16 >> (i & 15) & 1)) {
                     if (!(hits16 >> (i & 15))) i |= 15;  // no match left in these 16
                     continue;
@@ -718,7 +743,8 @@ int walk_keys(const uint8_t start[32], uint64_t count, uint8_t* keys) {
     if (w.init(start) != LXMFV_OK) return LXMFV_ERR_STATE;
     for (uint64_t done = 0; done < count;) {
         uint64_t first;
-        const uint8_t(*g)[32] = w.next_group(&first);
+        w.advance(&first);
+        const uint8_t(*g)[32] = w.keys();
         const uint64_t len = std::min<uint64_t>(W::SIZE, count - done);
         memcpy(keys + 32 * done, g, 32 * (size_t)len);
         done += len;

@@ -597,15 +597,22 @@ LXCPU_X16 __attribute__((always_inline)) inline void block3_shared(const V ih[4]
 #undef LXCPU_X16_K
 #undef LXCPU_X16_C
 
+// The first four destination-hash words of 16 keys that share the ed_pub and
+// name hash in k, from their x_pub words (big-endian, one key per lane).
+LXCPU_X16 __attribute__((always_inline)) inline void address16_shared_core(const V xw[8], const Shared16& k, V out[4]) {
+    V s[8];
+    block1_shared(xw, k, s);
+    compress_pad64(s);
+    block3_shared(s, k, out);
+}
+
 // address16 for 16 keys that share the ed_pub and name hash in k.
 LXCPU_X16 inline void address16_shared(const uint8_t* x, int x_stride, const Shared16& k, V out[4]) {
     const V lane = _mm512_set_epi32(15, 14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0);
     const V xoff = _mm512_mullo_epi32(lane, _mm512_set1_epi32(x_stride));
-    V xw[8], s[8];
+    V xw[8];
     for (int j = 0; j < 8; j++) xw[j] = bswap(_mm512_i32gather_epi32(xoff, (const void*)(x + 4 * j), 1));
-    block1_shared(xw, k, s);
-    compress_pad64(s);
-    block3_shared(s, k, out);
+    address16_shared_core(xw, k, out);
 }
 
 LXCPU_X16 inline void address16_shared_bytes(const uint8_t* x, int x_stride, const Shared16& k, uint8_t* out) {
@@ -627,6 +634,21 @@ LXCPU_X16 inline uint32_t match16_shared(const uint8_t* x, int x_stride, const S
                                          const uint32_t mask[4]) {
     V h[4];
     address16_shared(x, x_stride, k, h);
+    __mmask16 m = 0xFFFF;
+    for (int i = 0; i < 4; i++)
+        if (mask[i])
+            m &= _mm512_cmpeq_epi32_mask(_mm512_and_si512(h[i], _mm512_set1_epi32((int)mask[i])),
+                                         _mm512_set1_epi32((int)want[i]));
+    return m;
+}
+
+// match16_shared with x_pub stored word-major: word j (little-endian) of key m
+// at words[j * stride + m], as the IFMA walk writes its keys; no gathers.
+LXCPU_X16 inline uint32_t match16_shared_words(const uint32_t* words, size_t stride, const Shared16& k,
+                                               const uint32_t want[4], const uint32_t mask[4]) {
+    V xw[8], h[4];
+    for (int j = 0; j < 8; j++) xw[j] = bswap(_mm512_loadu_si512((const void*)(words + j * stride)));
+    address16_shared_core(xw, k, h);
     __mmask16 m = 0xFFFF;
     for (int i = 0; i < 4; i++)
         if (mask[i])
