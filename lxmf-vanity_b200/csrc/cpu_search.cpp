@@ -378,23 +378,20 @@ LXCPU_IFMA inline FV bcast(const F& a) {
 }
 LXCPU_IFMA inline V times19(V x) { return _mm512_add_epi64(_mm512_add_epi64(_mm512_slli_epi64(x, 4), _mm512_slli_epi64(x, 1)), x); }
 
-// As the scalar carry: limbs below 2^63 in, limb 1 at most 2^51 and the
-// others below 2^51 out.
+// One carry step on every limb at once (no ripple): limbs below 2^63 in;
+// limb i keeps its low 51 bits plus limb i-1's carry (limb 0: 19 times limb
+// 4's), so below 2^51 + 2^17 out, inside the multiplier's 52 bits.
 LXCPU_IFMA inline FV carry(FV a) {
     const V m = _mm512_set1_epi64((long long)MASK51);
-    for (int i = 0; i < 4; i++) {
-        a.l[i + 1] = _mm512_add_epi64(a.l[i + 1], _mm512_srli_epi64(a.l[i], 51));
-        a.l[i] = _mm512_and_si512(a.l[i], m);
-    }
-    const V c = _mm512_srli_epi64(a.l[4], 51);
-    a.l[4] = _mm512_and_si512(a.l[4], m);
-    a.l[0] = _mm512_add_epi64(a.l[0], times19(c));
-    a.l[1] = _mm512_add_epi64(a.l[1], _mm512_srli_epi64(a.l[0], 51));
-    a.l[0] = _mm512_and_si512(a.l[0], m);
+    V c[5];
+    for (int i = 0; i < 5; i++) c[i] = _mm512_srli_epi64(a.l[i], 51);
+    for (int i = 0; i < 5; i++) a.l[i] = _mm512_and_si512(a.l[i], m);
+    a.l[0] = _mm512_add_epi64(a.l[0], times19(c[4]));
+    for (int i = 1; i < 5; i++) a.l[i] = _mm512_add_epi64(a.l[i], c[i - 1]);
     return a;
 }
 
-// a + b without the carry: limbs up to 2^52 + 2^51, fit only for sub's b.
+// a + b without the carry: limbs below 2^52 + 2^18, fit only for sub's b.
 LXCPU_IFMA inline FV add_loose(const FV& a, const FV& b) {
     FV r;
     for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(a.l[k], b.l[k]);
@@ -458,8 +455,8 @@ LXCPU_IFMA inline FV sqr(const FV& a) {
 
 // The canonical encodings of the eight lanes as four little-endian 64-bit
 // words each (w[i] lane j), as the scalar to_bytes.  Limbs below 2^63 in: one
-// carry leaves a value below 2^255 + 2^52 < 2p, where q = [a >= p] is the
-// carry out of a + 19.
+// carry leaves a value below 2^255 + 2^222 < 2p, where q = [a >= p] is the
+// carry out of a + 19 (rippled through the limbs); the last pass ripples.
 LXCPU_IFMA inline void to_words(FV a, V w[4]) {
     a = carry(a);
     const V m = _mm512_set1_epi64((long long)MASK51);
