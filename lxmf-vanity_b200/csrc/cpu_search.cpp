@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -574,9 +575,10 @@ struct WalkIfma {
     static constexpr int SIZE = 2 * ifma::M;
     F uc, vc;
     uint64_t next = 0;
-    std::unique_ptr<ifma::Scratch> s{new ifma::Scratch};
+    std::unique_ptr<ifma::Scratch> s{new (std::nothrow) ifma::Scratch};  // about 170 KB
 
     int init(const uint8_t k[32]) {
+        if (!s) return LXMFV_ERR_STATE;  // out of memory: an error code, never an exception
         F pu, pv;
         if (int rc = start_point(k, pu, pv)) return rc;
         const ifma::Table& t = ifma::table();
