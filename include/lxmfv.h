@@ -315,7 +315,9 @@ int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* keys);
  * scalar draw, first_walker <= 2^24) with the identity's Ed25519 seed.
  * *tries (may be NULL) is updated every 10 ms with the keys tried.  Writes
  * the rechecked 64-byte identity and returns LXMFV_OK; LXMFV_STOPPED when
- * stopped without a hit; LXMFV_ERR_RECHECK when a hit failed its recheck.
+ * stopped without a hit; LXMFV_ERR_RECHECK when a hit failed its recheck;
+ * LXMFV_ERR_NOMEM when memory or threads ran out (threads already started are
+ * stopped and joined first).
  * LXMFV_CPU_HASH=c, =ni or =x16 picks the SHA-256 code (portable C, the SHA
  * extensions, AVX-512F) instead of the fastest; LXMFV_ERR_STATE where the
  * CPU lacks it. */

@@ -578,7 +578,7 @@ struct WalkIfma {
     std::unique_ptr<ifma::Scratch> s{new (std::nothrow) ifma::Scratch};  // about 170 KB
 
     int init(const uint8_t k[32]) {
-        if (!s) return LXMFV_ERR_STATE;  // out of memory: an error code, never an exception
+        if (!s) return LXMFV_ERR_NOMEM;  // an error code, never an exception
         F pu, pv;
         if (int rc = start_point(k, pu, pv)) return rc;
         const ifma::Table& t = ifma::table();
@@ -826,9 +826,9 @@ extern "C" int lxmfv_cpu_walk(const uint8_t start[32], uint64_t count, uint8_t* 
     }
 }
 
-extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
-                                const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
-                                uint8_t identity[64]) {
+static int cpu_search_body(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
+                           const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
+                           uint8_t identity[64]) {
     if (!prefix || nibbles < 1 || nibbles > 32 || !name_hash || threads < 1 || threads > LXMFV_CPU_MAX_THREADS ||
         !stop || !identity)
         return LXMFV_ERR_ARG;
@@ -901,7 +901,16 @@ extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uin
 #endif
     if (!run)
         run = hash == HASH_X16 ? walker<HASH_X16, Walk> : hash == HASH_NI ? walker<HASH_NI, Walk> : walker<HASH_C, Walk>;
-    for (int t = 0; t < threads; t++) pool.emplace_back(run, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
+    for (int t = 0; t < threads; t++) {
+        try {
+            pool.emplace_back(run, &s, &starts[32 * (size_t)t], &eds[32 * (size_t)t]);
+        } catch (...) {
+            // No more threads (a process limit, or memory): the ones started
+            // see the error, stop, and are joined below.
+            s.error.store(LXMFV_ERR_NOMEM);
+            break;
+        }
+    }
     while (!stopped(s)) {
         if (tries) __atomic_store_n(tries, s.tries.load(std::memory_order_relaxed), __ATOMIC_RELAXED);
         std::this_thread::sleep_for(std::chrono::milliseconds(10));
@@ -910,4 +919,18 @@ extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uin
     if (tries) __atomic_store_n(tries, s.tries.load(), __ATOMIC_RELAXED);
     if (s.error.load()) return s.error.load();
     return s.found.load() ? LXMFV_OK : LXMFV_STOPPED;
+}
+
+// No exception crosses the C ABI: an allocation failure before any thread
+// starts becomes LXMFV_ERR_NOMEM (thread creation is handled in the body).
+extern "C" int lxmfv_cpu_search(const uint8_t prefix[16], int nibbles, const uint8_t name_hash[10], int threads,
+                                const uint64_t* seed, uint64_t first_walker, const int* stop, uint64_t* tries,
+                                uint8_t identity[64]) {
+    try {
+        return cpu_search_body(prefix, nibbles, name_hash, threads, seed, first_walker, stop, tries, identity);
+    } catch (const std::bad_alloc&) {
+        return LXMFV_ERR_NOMEM;
+    } catch (...) {
+        return LXMFV_ERR_STATE;
+    }
 }

@@ -315,9 +315,28 @@ int capture_step(lxmfv_pool* p, uint32_t groups) {
 
 }  // namespace
 
+// No exception crosses the C ABI: a host allocation failure (the chunk tables
+// and lane maps grow with the capacity, up to 2^28 lanes) becomes
+// LXMFV_ERR_NOMEM, with a message when the pool exists (*pp, read after the
+// body ran: lxmfv_pool_open hands its pool out before it can fail).
+template <class Fn>
+static int no_throw(lxmfv_pool* const* pp, Fn&& body) noexcept {
+    const char* msg = "unexpected exception";
+    int rc = LXMFV_ERR_STATE;
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        msg = "out of host memory";
+        rc = LXMFV_ERR_NOMEM;
+    } catch (...) {
+    }
+    if (pp && *pp) try { (*pp)->err = msg; } catch (...) {}
+    return rc;
+}
+
 extern "C" {
 
-int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out) {
+static int pool_open_body(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     if (!out) return LXMFV_ERR_ARG;
     *out = nullptr;
     lxmfv_pool* p = new (std::nothrow) lxmfv_pool();
@@ -421,7 +440,7 @@ int lxmfv_pool_info(const lxmfv_pool* p, lxmfv_pool_info_t* info) {
     return LXMFV_OK;
 }
 
-int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* d, const uint8_t* scalars, uint32_t* search_id) {
+static int pool_submit_body(lxmfv_pool* p, const lxmfv_search_desc* d, const uint8_t* scalars, uint32_t* search_id) {
     if (!p || !d || !scalars || !search_id) return pfail(p, LXMFV_ERR_ARG, "null argument");
     if (d->lanes == 0 || d->lanes % 32) return pfail(p, LXMFV_ERR_ARG, "lanes %u: a positive multiple of 32", d->lanes);
     const uint32_t need = d->lanes / 32;
@@ -485,7 +504,7 @@ int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* d, const uint8_t* 
     return LXMFV_OK;
 }
 
-int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id) {
+static int pool_retire_body(lxmfv_pool* p, uint32_t search_id) {
     if (!p) return LXMFV_ERR_ARG;
     if (search_id >= p->max_searches || !p->searches[search_id].active)
         return pfail(p, LXMFV_ERR_ARG, "search %u is not active", search_id);
@@ -502,7 +521,7 @@ int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id) {
     return LXMFV_OK;
 }
 
-int lxmfv_pool_step(lxmfv_pool* p, uint32_t groups) {
+static int pool_step_body(lxmfv_pool* p, uint32_t groups) {
     if (!p) return LXMFV_ERR_ARG;
     if (groups == 0 || groups > (1u << 16)) return pfail(p, LXMFV_ERR_ARG, "groups %u: 1 .. 65536", groups);
     PCU(p, cudaSetDevice(p->device));
@@ -551,6 +570,22 @@ float lxmfv_pool_last_step_ms(const lxmfv_pool* p) {
     if (cudaEventSynchronize(p->ev1) != cudaSuccess) return -1.0f;
     if (cudaEventElapsedTime(&ms, p->ev0, p->ev1) != cudaSuccess) return -1.0f;
     return ms;
+}
+
+int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out) {
+    return no_throw(out, [&] { return pool_open_body(opts, out); });
+}
+
+int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* d, const uint8_t* scalars, uint32_t* search_id) {
+    return no_throw(&p, [&] { return pool_submit_body(p, d, scalars, search_id); });
+}
+
+int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id) {
+    return no_throw(&p, [&] { return pool_retire_body(p, search_id); });
+}
+
+int lxmfv_pool_step(lxmfv_pool* p, uint32_t groups) {
+    return no_throw(&p, [&] { return pool_step_body(p, groups); });
 }
 
 void lxmfv_pool_close(lxmfv_pool* p) {
