@@ -416,41 +416,51 @@ LXCPU_IFMA inline FV sub(const FV& a, const FV& b) { return carry(sub_loose(a, b
 
 // a * b mod p.  A 52 x 52-bit product splits at bit 52: its low half goes to
 // column i + j and its high half, worth 2^52 = 2 * 2^51, to column i + j + 1
-// doubled (the high halves are summed apart and doubled once).  Columns 5..9
-// fold down with 2^255 = 19.  Column bounds: 5 low + 10 high halves < 2^56;
-// after the fold below 2^62.
+// doubled.  Columns are built one at a time (its low halves, then the high
+// halves from the column below, doubled), so that few accumulators are live;
+// columns 5..9 fold down with 2^255 = 19.  Column bounds: 5 low + 10 high
+// halves < 2^56; after the fold below 2^62.
 LXCPU_IFMA inline FV mul(const FV& a, const FV& b) {
-    V lo[10], hi[10];
-    for (int k = 0; k < 10; k++) lo[k] = hi[k] = _mm512_setzero_si512();
-    for (int i = 0; i < 5; i++)
-        for (int j = 0; j < 5; j++) {
-            lo[i + j] = _mm512_madd52lo_epu64(lo[i + j], a.l[i], b.l[j]);
-            hi[i + j + 1] = _mm512_madd52hi_epu64(hi[i + j + 1], a.l[i], b.l[j]);
+    V z[10];
+#pragma GCC unroll 10
+    for (int k = 0; k < 10; k++) {
+        V lo = _mm512_setzero_si512(), hi = _mm512_setzero_si512();
+#pragma GCC unroll 5
+        for (int i = 0; i < 5; i++) {
+            if (k - i >= 0 && k - i < 5) lo = _mm512_madd52lo_epu64(lo, a.l[i], b.l[k - i]);
+            if (k - 1 - i >= 0 && k - 1 - i < 5) hi = _mm512_madd52hi_epu64(hi, a.l[i], b.l[k - 1 - i]);
         }
-    for (int k = 1; k < 10; k++) lo[k] = _mm512_add_epi64(lo[k], _mm512_slli_epi64(hi[k], 1));
+        z[k] = _mm512_add_epi64(lo, _mm512_slli_epi64(hi, 1));
+    }
     FV r;
-    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(lo[k], times19(lo[k + 5]));
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(z[k], times19(z[k + 5]));
     return carry(r);
 }
 
-// a^2: the cross products once, doubled.
+// a^2, column by column: the squares once and the cross products once,
+// doubled (column k = lo + 2 hi of the squares, 2 lo + 4 hi of the cross
+// products).
 LXCPU_IFMA inline FV sqr(const FV& a) {
-    V lo[10], hi[10], xlo[10], xhi[10];
-    for (int k = 0; k < 10; k++) lo[k] = hi[k] = xlo[k] = xhi[k] = _mm512_setzero_si512();
-    for (int i = 0; i < 5; i++) {
-        lo[2 * i] = _mm512_madd52lo_epu64(lo[2 * i], a.l[i], a.l[i]);
-        hi[2 * i + 1] = _mm512_madd52hi_epu64(hi[2 * i + 1], a.l[i], a.l[i]);
-        for (int j = i + 1; j < 5; j++) {
-            xlo[i + j] = _mm512_madd52lo_epu64(xlo[i + j], a.l[i], a.l[j]);
-            xhi[i + j + 1] = _mm512_madd52hi_epu64(xhi[i + j + 1], a.l[i], a.l[j]);
+    V z[10];
+#pragma GCC unroll 10
+    for (int k = 0; k < 10; k++) {
+        V sq = _mm512_setzero_si512(), cr = _mm512_setzero_si512();
+        if ((k & 1) == 0 && k / 2 < 5) sq = _mm512_madd52lo_epu64(sq, a.l[k / 2], a.l[k / 2]);
+        if ((k & 1) == 1 && (k - 1) / 2 < 5)
+            sq = _mm512_add_epi64(sq, _mm512_slli_epi64(
+                                          _mm512_madd52hi_epu64(_mm512_setzero_si512(), a.l[(k - 1) / 2], a.l[(k - 1) / 2]), 1));
+        V xl = _mm512_setzero_si512(), xh = _mm512_setzero_si512();
+#pragma GCC unroll 5
+        for (int i = 0; i < 5; i++) {
+            const int j = k - i, jh = k - 1 - i;
+            if (j > i && j < 5) xl = _mm512_madd52lo_epu64(xl, a.l[i], a.l[j]);
+            if (jh > i && jh < 5) xh = _mm512_madd52hi_epu64(xh, a.l[i], a.l[jh]);
         }
+        cr = _mm512_add_epi64(_mm512_slli_epi64(xl, 1), _mm512_slli_epi64(xh, 2));
+        z[k] = _mm512_add_epi64(sq, cr);
     }
-    // column k = lo + 2 hi + 2 xlo + 4 xhi
-    for (int k = 0; k < 10; k++)
-        lo[k] = _mm512_add_epi64(_mm512_add_epi64(lo[k], _mm512_slli_epi64(xlo[k], 1)),
-                                 _mm512_slli_epi64(_mm512_add_epi64(hi[k], _mm512_slli_epi64(xhi[k], 1)), 1));
     FV r;
-    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(lo[k], times19(lo[k + 5]));
+    for (int k = 0; k < 5; k++) r.l[k] = _mm512_add_epi64(z[k], times19(z[k + 5]));
     return carry(r);
 }
 
