@@ -6,20 +6,25 @@ aspect lxmf.delivery, every lane starting from its own seeded clamped X25519
 scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, 2^36 keys
 walked in total over the timed steps (a step is one launch that walks every
 lane `iters` groups further).  Keys per inversion: the tuned 512 for the
-headline, and a second measurement at 64 (the reference kernel's BATCH) on a
-quarter of the keys.  Synthetic, seeded inputs; no dataset is involved.
+headline; the same 2^36 keys again at 64 (the reference kernel's BATCH), with
+the grouped walk (`at_batch_64`) and with the x-only walk, the reference's
+algorithm (`xadd_b64`).  Synthetic, seeded inputs; no dataset is involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line on rank 0.  `value` is device-timed (CUDA events on the
-launching stream, max over ranks), `e2e` goes through the C ABI's
-synchronous lxmfv_launch with host buffers, `cpu_baseline` is the restated
-CPU search on this host's cores, `roofline` relates the walk kernel's
-ALU-pipe work (ncu counts per key) to the measured ALU rate of this GPU, and
-`reference_cuda_kernel` times the reference's own CUDA kernel on this GPU and
-`cpu_search` this library's CPU search (the reference's default mode).
-With --impl reference, the reference's own kernel body (src/gpu/common.h,
-built for the host) is timed on the host cores instead.
+With --gpus N > 1 and no launcher around it, bench.py starts its N ranks
+itself under torch.distributed.run (one process per GPU); under a launcher
+the world size must equal N.  Prints one JSON line on rank 0.  `value` is
+device-timed (CUDA events on the launching stream, max over ranks), `e2e`
+goes through the C ABI's synchronous lxmfv_launch with host buffers,
+`cpu_baseline` is the restated CPU search on this host's cores, `roofline`
+relates the walk kernel's ALU-pipe work (ncu counts per key) to the measured
+ALU rate of this GPU (and `roofline.imad_ncu` its IMAD-class instructions to
+the measured IMAD rate), `reference_cuda_kernel` times the reference's own
+CUDA kernel on this GPU and `cpu_search` this library's CPU search (the
+reference's default mode).  With --impl reference, the reference's own
+kernel body (src/gpu/common.h, built for the host) is timed on the host
+cores instead.
 """
 from __future__ import annotations
 
@@ -85,7 +90,10 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-cpu-search", action="store_true", help="skip timing this library's CPU search")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA kernel")
-    p.add_argument("--no-b64", action="store_true", help="skip the second measurement at B = 64")
+    p.add_argument("--no-b64", action="store_true", help="skip the measurements at B = 64 (grouped and x-only walks)")
+    p.add_argument("--engine", default="gpu",
+                   help="gpu (the CUDA kernels, NCCL between ranks), or module:function, a host-side stand-in "
+                        "measured over gloo that the launcher's tests use")
     p.add_argument("--no-batched", action="store_true", help="skip the 256-search batched measurement")
     p.add_argument("--served-seconds", type=float, default=60.0,
                    help="length of the served-requests run (0: skip); the full served workload is 600")
@@ -263,7 +271,7 @@ def batched_workload(lx, dev: int, single_value: float) -> dict:
     import lxmfv_serve as srv
     specs = srv.batched_specs(256, seed=4, lanes=1184, min_nibbles=4, max_nibbles=10)
     with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=512) as pool:
-        r = srv.run_batched(pool, specs, steps=6, groups=4, warmup=1, recheck_limit=8)
+        r = srv.run_batched(pool, specs, steps=6, groups=4, warmup=1)  # every hit rechecked
     r["vs_single_search"] = r["keys_per_s"] / single_value
     r["workload"] = "256 searches, 4-10 nibbles, 3 aspects, 1184 lanes each, one persistent launch per step"
     return r
@@ -284,9 +292,38 @@ def served_workload(dev: int, seconds: float) -> dict:
     return out
 
 
+def relaunch(n: int) -> int:
+    """--gpus N > 1 without a launcher: start N ranks of this same command line
+    under torch.distributed.run, one process per GPU, rendezvous on
+    127.0.0.1; returns the launcher's exit code (non-zero if any rank
+    failed).  Only rank 0 prints the JSON line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def gather_ranks(dist, world: int, rec: dict) -> list[dict]:
+    """Every rank's record, in rank order, on every rank (one all-gather)."""
+    if world == 1:
+        return [rec]
+    out: list = [None] * world
+    dist.all_gather_object(out, rec)
+    return out
+
+
 def main() -> None:
     a = parse()
+    if a.gpus < 1:
+        sys.exit("bench.py: --gpus must be at least 1")
+    if "WORLD_SIZE" not in os.environ and a.gpus > 1:
+        sys.exit(relaunch(a.gpus))
     world, rank, local = dist_setup()
+    if world != a.gpus:
+        sys.exit(f"bench.py: --gpus {a.gpus} does not match the {world} rank(s) launched")
     if a.impl == "reference":
         if rank != 0:
             return
@@ -302,11 +339,16 @@ def main() -> None:
                 "e2e": {"value": ref["value"], "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+    if a.engine != "gpu":
+        host_engine_main(a, world, rank)
+        return
 
     import torch
     import torch.distributed as dist
 
     import lxmfv as lx
+    if torch.cuda.device_count() < world:
+        sys.exit(f"bench.py: {world} ranks need {world} GPUs; {torch.cuda.device_count()} visible")
     dev = local
     torch.cuda.set_device(dev)  # before the process group, so each rank's NCCL communicator uses its own GPU
     if world > 1:
@@ -314,6 +356,7 @@ def main() -> None:
     prefix = _prefix()
     head = measure(torch, dist, lx, a, dev, rank, world, prefix, a.walk, a.batch, a.total_keys, a.steps, a.warmup,
                    e2e=not a.no_e2e)
+    ranks = gather_ranks(dist, world, head["rank_record"])
     line = {
         "metric": METRIC, "value": head["value"], "unit": "keys/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -324,38 +367,77 @@ def main() -> None:
         "roofline": head["roofline"],
         "clocks": head["clocks"],
         "hits": head["hits"],
+        "ranks": ranks,
         "start_points_s": head["start_points_s"],
     }
-    if not a.no_b64 and a.batch != 64:
-        # The same workload at B = 64 keys per inversion, the reference kernel's
-        # batch (2^34 keys: a quarter of the headline's, to bound the run time).
-        b64 = measure(torch, dist, lx, a, dev, rank, world, prefix, a.walk, 64, a.total_keys / 4, a.steps,
-                      a.warmup, e2e=False)
-        line["at_batch_64"] = {"value": b64["value"], "unit": "keys/s", "ms_per_step": b64["ms_per_step"],
-                               "config": b64["config"], "clocks": b64["clocks"], "hits": b64["hits"]}
+    bad = head["hits"]["rechecked_bad"]
     # The side sections run once, on a single-GPU run (rank 0 of world 1).
-    if rank == 0 and world == 1 and not a.no_batched:
+    single = rank == 0 and world == 1
+    if single and not a.no_b64 and a.batch != 64:
+        # The same workload at B = 64 keys per inversion, the reference kernel's
+        # batch: the grouped walk, then the x-only walk (the reference's
+        # algorithm: xADD by Q and Montgomery batch inversion over 64 keys).
+        for key, walk in (("at_batch_64", "group"), ("xadd_b64", "xadd")):
+            r = measure(torch, dist, lx, a, dev, rank, world, prefix, walk, 64, a.total_keys, a.steps, a.warmup,
+                        e2e=False)
+            line[key] = {"value": r["value"], "unit": "keys/s", "ms_per_step": r["ms_per_step"],
+                         "gpu_launches": a.steps, "config": r["config"], "roofline": r["roofline"],
+                         "clocks": r["clocks"], "hits": r["hits"]}
+            bad += r["hits"]["rechecked_bad"]
+    if single and not a.no_batched:
         line["batched"] = batched_workload(lx, dev, head["value"])
-    if rank == 0 and world == 1 and a.served_seconds > 0:
+        bad += line["batched"]["rechecked_bad"]
+    if single and a.served_seconds > 0:
         line["served"] = served_workload(dev, a.served_seconds)
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        bad += line["served"]["rechecked_bad"]
+    if single and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(prefix)
-    if rank == 0 and world == 1 and not a.no_cpu_search:
+    if single and not a.no_cpu_search:
         line["cpu_search"] = cpu_search_rate()
-    if rank == 0 and world == 1 and not a.no_ref_cuda:
+    if single and not a.no_ref_cuda:
         with lx.Backend(device=dev, lanes=1024) as b:
             line["reference_cuda_kernel"] = reference_cuda_kernel(b, lx, prefix)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if head["hits"]["rechecked_bad"]:
-        sys.exit(f"{head['hits']['rechecked_bad']} GPU hits failed their CPU recheck")
+    if bad:
+        sys.exit(f"{bad} GPU hits failed their CPU recheck")
+
+
+def host_engine_main(a, world: int, rank: int) -> None:
+    """The multi-rank plumbing of the GPU run (rank seeds, max-over-ranks
+    timing, the whole-job rate, one line from rank 0) around a host-side
+    engine `module:function`, with gloo between the ranks.  The function is
+    called as f(seed=, steps=, warmup=, prefix=, lanes=) and returns
+    {"keys_per_step": K, "ms": device-or-wall milliseconds of the timed steps,
+    "hits": [(lane, n), ...]}."""
+    import datetime
+    import importlib
+
+    import torch.distributed as dist
+    mod, _, fn = a.engine.partition(":")
+    f = getattr(importlib.import_module(mod), fn)
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    seed = replicas.rank_seed(SEED, rank)
+    prefix = _prefix()
+    r = f(seed=seed, steps=a.steps, warmup=a.warmup, prefix=prefix, lanes=a.lanes or 4)
+    ms = replicas.max_over_ranks(dist, r["ms"], "cpu")
+    value = replicas.aggregate_rate(r["keys_per_step"] * a.steps, ms * 1e-3, world)
+    ranks = gather_ranks(dist, world, {"rank": rank, "seed": seed, "ms": r["ms"], "hits": [list(h) for h in r["hits"]]})
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": world, "steps": a.steps,
+                          "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+                          "scaling": "weak", "engine": a.engine, "prefix": prefix, "ranks": ranks}), flush=True)
 
 
 def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_keys, steps, warmup, e2e=True) -> dict:
     """Times `steps` launches (after `warmup`) of the walk over `total_keys`
-    keys in all, device-timed with CUDA events on the launching stream."""
+    keys in all, device-timed with CUDA events on the launching stream; every
+    hit is rechecked from scratch on the CPU."""
     walk_id = lx.WALK_GROUP if walk == "group" else lx.WALK_XADD
     # A stream of our own (never the legacy default stream, whose handle is 0):
     # the library launches on it and the timing events are recorded on it.
@@ -387,9 +469,9 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
             b.launch_async(args)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = ev0.elapsed_time(ev1)
+    ms_rank = ev0.elapsed_time(ev1)
     hits, n_hits = b.collect()
-    ms = replicas.max_over_ranks(dist, ms, f"cuda:{dev}")
+    ms = replicas.max_over_ranks(dist, ms_rank, f"cuda:{dev}")
     value = replicas.aggregate_rate(keys_per_step * steps, ms * 1e-3, world)
 
     # Every hit is rechecked from scratch on the CPU (OpenSSL), as the reference does.
@@ -438,15 +520,26 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
                     "issue": {"achieved": ncu["inst"] * keys_per_s_kernel / 1e12, "peak": issue_peak / 1e12,
                               "unit": "T inst/s", "frac": ncu["inst"] * keys_per_s_kernel / issue_peak},
                     "imad": imad_line}
+        if "imad" in ncu:
+            # The metric's own IMAD fraction: IMAD-class instructions per key
+            # from ncu (every IMAD variant: .HI, .WIDE, .X, .MOV, .SHL) x keys/s
+            # over the measured mad.lo.u32 rate.
+            imad_ncu = ncu["imad"] * keys_per_s_kernel
+            roofline["imad_ncu"] = {"achieved": imad_ncu / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
+                                    "frac": imad_ncu / imad_peak, "per_key": ncu["imad"],
+                                    "note": "ncu sass__inst_executed_per_opcode, opcode IMAD (all variants), "
+                                            "x 32 lanes / keys; peak = measured mad.lo.u32 rate of this GPU"}
     else:
         roofline = dict(imad_line, bound="imad", traffic=None, alu_peak=alu_peak / 1e12)
     config = {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, seeded walkers, 2^36 keys per run)",
               "walk": walk, "prefix": prefix, "lanes_per_gpu": lanes, "batch": batch, "iters_per_step": iters,
               "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
               "l2": "working set (lane state + per-lane batch buffers) exceeds L2; no flush needed"}
+    rank_record = {"rank": rank, "device": dev, "seed": replicas.rank_seed(SEED, rank), "ms": ms_rank,
+                   "keys": keys_per_step * steps, "hits": int(n_hits), "rechecked_bad": len(bad)}
     return {"value": value, "ms_per_step": ms / steps, "e2e": e2e_line, "roofline": roofline,
-            "clocks": clk.summary(), "hits": {"found": int(n_hits), "rechecked_bad": len(bad)},
-            "start_points_s": ladder_s, "config": config}
+            "clocks": clk.summary(), "hits": {"found": int(n_hits), "rechecked": len(hits), "rechecked_bad": len(bad)},
+            "start_points_s": ladder_s, "config": config, "rank_record": rank_record}
 
 
 def _prefix() -> str:

@@ -15,8 +15,9 @@ to search for many prefixes it starts many processes.  Here:
 - `serve` is a request loop: searches arrive (a Poisson stream), are admitted
   while the pool has lanes for them (the memory budget), and are retired on
   their first hit, which frees lanes for the next ones while the others keep
-  walking (continuous batching).  It reports time-to-hit percentiles
-  normalised by each search's expected work.
+  walking (continuous batching).  It reports wall-clock time-to-hit
+  percentiles normalised by each search's expected time at its measured
+  rate, beside the same in keys walked.
 """
 from __future__ import annotations
 
@@ -177,9 +178,11 @@ def batched_specs(n: int, seed: int, lanes: int, min_nibbles: int = 4, max_nibbl
 
 
 def run_batched(pool: Pool, specs: list[SearchSpec], steps: int, groups: int, warmup: int = 1,
-                recheck_limit: int = 64) -> dict:
+                recheck_limit: int | None = None) -> dict:
     """Walks every search for `warmup` + `steps` steps, device-timing the
-    steps; every search's first hits (up to recheck_limit each) are rechecked."""
+    steps; every hit of the timed steps is rechecked from scratch on the CPU
+    (with recheck_limit, only each search's first that many: the autotuner's
+    quick sweeps)."""
     sids = [pool.submit(s) for s in specs]
     for _ in range(warmup):
         pool.step(groups)
@@ -199,7 +202,7 @@ def run_batched(pool: Pool, specs: list[SearchSpec], steps: int, groups: int, wa
     checked = 0
     for sid, lane, n in hits_all:
         c = per_search.get(sid, 0)
-        if c < recheck_limit:
+        if recheck_limit is None or c < recheck_limit:
             checked += 1
             bad += 0 if pool.specs[sid].recheck(lane, n) else 1
         per_search[sid] = c + 1
@@ -288,6 +291,7 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
     steps = 0
     keys = 0
     busy_ms = 0.0
+    step_wall = 0.0  # wall time of the loop's step + poll calls
     bad = 0
     while pending or waiting or active:
         now = time.perf_counter() - t0
@@ -317,11 +321,13 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
                 time.sleep(max(0.0, min(pending[0].arrival - now, 0.05)))
             continue
         lanes = sum(r.spec.lanes for r in active.values())
+        t_step = time.perf_counter()
         pool.step(groups)
         hits, _ = pool.poll()
         steps += 1
         keys += lanes * pool.batch * groups
         busy_ms += pool.last_step_ms()
+        step_wall += time.perf_counter() - t_step
         t_now = time.perf_counter() - t0
         first: dict[int, tuple[int, int]] = {}
         for sid, lane, n in hits:
@@ -344,26 +350,56 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
             pool.retire(sid)
             done.append(r)
     wall = time.perf_counter() - t0
-    return summarise(done, requests, wall, keys, busy_ms, steps, bad, failed=len(failed))
+    lane_rate = steps * pool.batch * groups / step_wall if step_wall > 0 else 0.0
+    return summarise(done, requests, wall, keys, busy_ms, steps, bad, failed=len(failed), lane_rate=lane_rate)
+
+
+def wall_time_to_hit(r: Request) -> float:
+    """A done request's wall-clock time to hit over its expected time at its
+    measured rate.  The time to hit runs from arrival (so it includes the
+    queue wait) to the poll that reported the hit (so it includes the rest of
+    that step).  The rate is the request's own: the keys it walked over its
+    wall time in the pool, arrival excluded, so a loaded pool's slower steps
+    are in the rate and the wait is in the time.  The expected time is then
+    16^L over that rate, and an exponential time to hit has the quantiles
+    ln 2, ln 20 and ln 100 at p50, p95 and p99."""
+    in_pool = r.done - r.admitted
+    if in_pool <= 0 or not r.walked:
+        return float("nan")
+    expected_s = expected_tries(r.spec.nibbles) * in_pool / r.walked
+    return (r.done - r.arrival) / expected_s
 
 
 def summarise(done: list[Request], requests: list[Request], wall: float, keys: int, busy_ms: float, steps: int,
-              bad: int, failed: int = 0) -> dict:
+              bad: int, failed: int = 0, lane_rate: float = 0.0) -> dict:
     norm_tries = np.array([r.tries / expected_tries(r.spec.nibbles) for r in done]) if done else np.zeros(0)
     # Time in service at the search's own (constant, per step) key rate is its
     # walked keys over that rate, so its time over the expected time is the
     # walked keys over the expected tries: the tries, rounded up to the end of
     # the step that reported the hit.
     norm_service = np.array([r.walked / expected_tries(r.spec.nibbles) for r in done]) if done else np.zeros(0)
+    # Wall clock: arrival to the reported hit, over 16^L at the request's own
+    # measured rate (wall_time_to_hit), and over 16^L at the pool's mean rate
+    # per lane (every step's keys per lane over the wall time of the steps)
+    # times the request's lanes.
+    norm_wall = np.array([wall_time_to_hit(r) for r in done]) if done else np.zeros(0)
+    norm_wall_pool = (np.array([(r.done - r.arrival) * r.spec.lanes * lane_rate / expected_tries(r.spec.nibbles)
+                                for r in done]) if done and lane_rate > 0 else np.zeros(0))
     rate = keys / (busy_ms * 1e-3) if busy_ms > 0 else 0.0
     q = lambda a, p: float(np.quantile(a, p)) if len(a) else float("nan")  # noqa: E731
     targets = {"p50": math.log(2), "p95": math.log(20), "p99": math.log(100)}
+    pct = (("p50", .5), ("p95", .95), ("p99", .99))
+    wall_q = {k: q(norm_wall, p) for k, p in pct}
     out = {
         "requests": len(requests), "done": len(done), "failed": failed, "wall_s": wall, "steps": steps,
         "aggregate_keys_per_s": rate, "busy_fraction": busy_ms * 1e-3 / wall if wall > 0 else 0.0,
         "rechecked_bad": bad,
-        "tries_over_expected": {k: q(norm_tries, p) for k, p in (("p50", .5), ("p95", .95), ("p99", .99))},
-        "service_time_over_expected": {k: q(norm_service, p) for k, p in (("p50", .5), ("p95", .95), ("p99", .99))},
+        "time_to_hit_over_expected": wall_q,
+        "time_to_hit_deviation": {k: wall_q[k] / targets[k] - 1 for k in wall_q},
+        "time_to_hit_at_pool_rate": {k: q(norm_wall_pool, p) for k, p in pct},
+        "lane_keys_per_s": lane_rate,
+        "tries_over_expected": {k: q(norm_tries, p) for k, p in pct},
+        "service_time_over_expected": {k: q(norm_service, p) for k, p in pct},
         "targets": targets,
         "latency_s": {k: q(np.array([r.done - r.arrival for r in done]), p) for k, p in (("p50", .5), ("p95", .95), ("p99", .99))},
         "queue_wait_s": {k: q(np.array([r.admitted - r.arrival for r in done]), p) for k, p in (("p50", .5), ("p99", .99))},

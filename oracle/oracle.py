@@ -9,6 +9,7 @@ as the timed CPU baseline, never as the thing measured on the GPU.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 import subprocess
 
@@ -27,9 +28,22 @@ _lib = None
 _ref = None
 
 
+def ref_dir() -> str:
+    """Where the reference tree is: $LXMFV_REF_DIR, else the reference_path
+    recorded in the repository's BASELINE.json, else '' (not available)."""
+    d = os.environ.get("LXMFV_REF_DIR", "")
+    if not d:
+        try:
+            with open(os.path.join(os.path.dirname(HERE), "BASELINE.json")) as f:
+                d = json.load(f).get("reference_path", "") or ""
+        except (OSError, ValueError):
+            d = ""
+    return d
+
+
 def build() -> None:
     """Compile the checkers (the reference shim only where the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={ref_dir()}"], check=True)
 
 
 def lib():
