@@ -344,19 +344,22 @@ int lxmfv_fe_op(lxmfv_handle* h, int op, const uint32_t* a, const uint32_t* b, u
 #define LXMFV_STATIC_SCRATCH_ELEMS 131072u
 
 /* The batch inversion of lxmfv_fe_op op 3 on device buffers the caller owns,
- * with no device allocation: for code that cannot call cudaMalloc (a stream
- * capture in progress, a host runtime that owns every device allocation, a
- * path where an allocation's synchronisation is not acceptable).  No
- * counterpart in the reference.
+ * with no device allocation: for callers that may not call cudaMalloc or
+ * cudaFree (a host runtime that owns every device allocation and hands the
+ * library its buffers, a loop that cannot take cudaFree's implicit device
+ * synchronisation).  No counterpart in the reference.
  * d_a, d_out: device pointers on the current device, 16-byte aligned,
  * `count` elements of 8 little-endian words (inputs drop bit 255, outputs are
- * canonical); group 1..256.  The kernel is enqueued on `stream` (NULL: the
- * default stream) and the call returns without waiting for it.
+ * canonical); group 1..256.  d_out may equal d_a (in place); ranges that
+ * overlap otherwise are rejected with LXMFV_ERR_ARG.  The kernel is enqueued
+ * on `stream` (NULL: the default stream) and the call returns without
+ * waiting for it.
  * The working storage is one static device array shared by every call:
  * count above LXMFV_STATIC_SCRATCH_ELEMS is rejected with LXMFV_ERR_ARG, and
  * calls whose kernels overlap on the GPU race on the array, so the caller
- * must order them.  The first call on a device looks up the array's device
- * address with that device current; make it before any stream capture.
+ * must order them.  The first call in a device's context looks up the
+ * array's device address with that device current; make it before any
+ * stream capture.  After cudaDeviceReset the next call looks it up again.
  * A message for a non-zero return goes to err (err_len bytes) when given. */
 int lxmfv_fe_batch_invert_static(const uint32_t* d_a, uint32_t* d_out, uint64_t count, uint32_t group, void* stream,
                                  char* err, size_t err_len);

@@ -408,11 +408,15 @@ static int pool_open_body(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     for (uint32_t c = 0; c < p->chunks; c++) p->free_chunks[c] = p->chunks - 1 - c;  // pop_back gives 0, 1, ...
     p->searches.resize(p->max_searches);
     // The grouped walk's table (as lxmfv_open builds it).
+    // Both scratch buffers are freed on every path, including a failed allocation of the second.
     fe *du = nullptr, *dv = nullptr;
-    PCU(p, cudaMalloc(&du, sizeof(fe) * (p->m + 1)));
-    PCU(p, cudaMalloc(&dv, sizeof(fe) * (p->m + 1)));
-    lxk::group_table_kernel<<<1, ((p->m + 1 + 31) / 32) * 32, 0, p->stream>>>(du, dv, p->m, pool_u8b(), pool_v8b());
-    e = cudaGetLastError();
+    e = cudaMalloc(&du, sizeof(fe) * (p->m + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dv, sizeof(fe) * (p->m + 1));
+    if (e == cudaSuccess) {
+        lxk::group_table_kernel<<<1, ((p->m + 1 + 31) / 32) * 32, 0, p->stream>>>(du, dv, p->m, pool_u8b(),
+                                                                                  pool_v8b());
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->tu, du, sizeof(fe) * (p->m + 1), cudaMemcpyDeviceToHost, p->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->tv, dv, sizeof(fe) * (p->m + 1), cudaMemcpyDeviceToHost, p->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
