@@ -47,7 +47,7 @@ typedef struct lxmfv_handle lxmfv_handle;
  *        with Montgomery's batch inversion over `batch` keys. */
 #define LXMFV_WALK_GROUP 0
 #define LXMFV_WALK_XADD 1
-#define LXMFV_MAX_HALF_GROUP 256
+#define LXMFV_MAX_HALF_GROUP 512
 
 /* Option flags.  PHASE_SYNC (grouped walk, blocks of 256 or 512): a block
  * barrier after every group keeps a block's warps in the same phase of the
@@ -65,7 +65,7 @@ typedef struct lxmfv_handle lxmfv_handle;
 typedef struct {
     int32_t device;       /* CUDA device ordinal */
     uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
-    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 512; 0: the fastest (GROUP 512, XADD 128) */
+    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 1024; 0: the fastest (GROUP 512, XADD 128) */
     uint32_t block;       /* threads per block: 128, 256 or 512; 0: 512 with LXMFV_FLAG_PHASE_SYNC */
     uint32_t walk;        /* LXMFV_WALK_GROUP (0, default) or LXMFV_WALK_XADD */
     uint32_t flags;       /* LXMFV_FLAG_* */

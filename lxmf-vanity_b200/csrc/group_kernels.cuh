@@ -22,6 +22,7 @@
 // of the group's first key.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "walk_kernels.cuh"
 
@@ -46,6 +47,38 @@ struct GroupArgs {
     EmitArgs em;
     GroupTable<M> t;
 };
+
+// G = 1024 (M = 512): the table (2 x 513 points, 33 KB) no longer fits the
+// kernel parameter block (32 KB), so it lives in constant memory, where the
+// warps read it through the same constant cache.  It depends on nothing but
+// M, so every handle on a device shares it; lxmfv_open writes it there.
+constexpr int kConstTableM = 512;
+static __device__ __constant__ fe c_group_u[kConstTableM + 1];
+static __device__ __constant__ fe c_group_v[kConstTableM + 1];
+struct ConstTableU {
+    __device__ __forceinline__ fe operator[](int i) const { return c_group_u[i]; }
+};
+struct ConstTableV {
+    __device__ __forceinline__ fe operator[](int i) const { return c_group_v[i]; }
+};
+struct ConstGroupTable {
+    ConstTableU u;
+    ConstTableV v;
+};
+struct GroupArgsConst {
+    uint32_t* state;
+    uint64_t* ns;
+    uint32_t lanes;
+    uint32_t iters;
+    EmitArgs em;
+};
+template <int M>
+__device__ __forceinline__ const GroupTable<M>& table_of(const GroupArgs<M>& a) { return a.t; }
+__device__ __forceinline__ ConstGroupTable table_of(const GroupArgsConst&) { return ConstGroupTable{}; }
+// The launch parameters of the grouped walk at M: the table travels in them
+// up to M = 256, and sits in constant memory above.
+template <int M>
+using GroupArgsFor = typename std::conditional<(M > 256), GroupArgsConst, GroupArgs<M>>::type;
 
 // y-coordinate recovery on a Montgomery curve (Okeya and Sakurai, CHES 2001;
 // the form of Costello and Smith, "Montgomery curves and their arithmetic",
@@ -140,8 +173,8 @@ static __global__ void __launch_bounds__(128) group_init_kernel(uint32_t* state,
 // phase of the walk, so that they share the instruction cache's working set
 // (one phase's code instead of all of it); every thread of the block must
 // then call this with the same `groups`.
-template <int M, bool SYNC, class Emit>
-__device__ __forceinline__ void walk_groups(fe& uc, fe& vc, uint64_t& n, uint32_t groups, const GroupTable<M>& t,
+template <int M, bool SYNC, class Table, class Emit>
+__device__ __forceinline__ void walk_groups(fe& uc, fe& vc, uint64_t& n, uint32_t groups, const Table& t,
                                             const Emit& emit) {
     fe pre[M + 1];
     fe cA = fe_zero();
@@ -211,8 +244,8 @@ struct LaneEmit {
 
 // Threads past the last lane walk a copy of the last lane and neither emit
 // nor store (with SYNC they must still reach every barrier).
-template <int M, int BLOCK, int MINB, bool SYNC, bool DUMP>
-static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ GroupArgs<M> a) {
+template <int M, int BLOCK, int MINB, bool SYNC, bool DUMP, class Args = GroupArgsFor<M>>
+static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __grid_constant__ Args a) {
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     if (!SYNC && tid >= a.lanes) return;
     const bool active = tid < a.lanes;
@@ -222,7 +255,7 @@ static __global__ void __launch_bounds__(BLOCK, MINB) group_walk_kernel(const __
     const uint64_t key0 = a.ns[lane];
     uint64_t n = key0;
     const LaneEmit<DUMP> emit{a.em, lane, key0, active};
-    walk_groups<M, SYNC>(uc, vc, n, a.iters, a.t, emit);
+    walk_groups<M, SYNC>(uc, vc, n, a.iters, table_of(a), emit);
     if (active) {
         store_fe(a.state, 0, lane, a.lanes, uc);
         store_fe(a.state, 1, lane, a.lanes, vc);

@@ -134,6 +134,7 @@ const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool 
             case 128: return group_kernel_ptr<64>(block, sync, low_regs, dump);
             case 256: return group_kernel_ptr<128>(block, sync, low_regs, dump);
             case 512: return group_kernel_ptr<256>(block, sync, low_regs, dump);
+            case 1024: return group_kernel_ptr<512>(block, sync, low_regs, dump);
         }
     }
     return nullptr;
@@ -149,18 +150,20 @@ void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
 
 template <int M>
 void launch_group(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
-    lxk::GroupArgs<M> ga;
+    lxk::GroupArgsFor<M> ga;
     ga.state = h->d_state;
     ga.ns = h->d_ns;
     ga.lanes = h->lanes;
     ga.iters = iters;
     ga.em = em;
-    for (int i = 0; i <= M; i++) {
-        ga.t.u[i] = h->tu[i];
-        ga.t.v[i] = h->tv[i];
+    if constexpr (M <= 256) {
+        for (int i = 0; i <= M; i++) {
+            ga.t.u[i] = h->tu[i];
+            ga.t.v[i] = h->tv[i];
+        }
     }
     const unsigned grid = (h->lanes + h->block - 1) / h->block;
-    typedef void (*fn_t)(lxk::GroupArgs<M>);
+    typedef void (*fn_t)(lxk::GroupArgsFor<M>);
     const fn_t fn = (fn_t)group_kernel_ptr<M>(h->block, h->sync, h->low_regs, em.dump_lanes > 0);
     fn<<<grid, h->block, 0, h->stream>>>(ga);
 }
@@ -187,7 +190,8 @@ void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const
             case 64: launch_group<32>(h, em, iters); break;
             case 128: launch_group<64>(h, em, iters); break;
             case 256: launch_group<128>(h, em, iters); break;
-            default: launch_group<256>(h, em, iters); break;
+            case 512: launch_group<256>(h, em, iters); break;
+            default: launch_group<512>(h, em, iters); break;
         }
     }
 }
@@ -293,6 +297,16 @@ int build_group_table(lxmfv_handle* h) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(du);
     cudaFree(dv);
+    if (e == cudaSuccess && m > 256) {
+        // The G = 1024 kernels read the table from constant memory.  Every
+        // handle on the device writes the same bytes, so a launch of another
+        // handle that reads it meanwhile sees no change.
+        e = cudaMemcpyToSymbolAsync(lxk::c_group_u, h->tu, sizeof(fe) * (m + 1), 0, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyToSymbolAsync(lxk::c_group_v, h->tv, sizeof(fe) * (m + 1), 0, cudaMemcpyHostToDevice,
+                                        h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
     if (e != cudaSuccess) return fail(h, LXMFV_ERR_CUDA, "group table: %s", cudaGetErrorString(e));
     return LXMFV_OK;
 }
@@ -326,7 +340,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
         return fail(h, LXMFV_ERR_ARG,
                     "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
-                    "batch 32, 64, 128, 256, 512; block 128, 256 or 512)",
+                    "batch 32, 64, 128, 256, 512, 1024; block 128, 256 or 512)",
                     h->batch, h->block);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);

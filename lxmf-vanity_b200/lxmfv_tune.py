@@ -4,7 +4,7 @@ Measures the plain search's keys/s for each launch configuration the library
 builds and returns the fastest:
 
   - the walk: grouped (default) or x-only (the reference's);
-  - keys per inversion: grouped G in {32, 64, 128, 256, 512}, x-only B in {16, 32, 64, 128};
+  - keys per inversion: grouped G in {32, 64, 128, 256, 512, 1024}, x-only B in {16, 32, 64, 128};
   - threads per block: 128, 256 or 512, with or without the phase barrier;
   - the register cap: 128 per thread (every kernel) or 80 (LXMFV_FLAG_REGCAP_80:
     grouped walk, G = 256, 256-thread blocks with the barrier, three blocks per SM);
@@ -55,7 +55,7 @@ def candidates(walks=("group", "xadd"), quick: bool = False) -> list[WalkConfig]
     out = []
     shapes = [(128, False), (256, False), (256, True), (512, False), (512, True)]
     if "group" in walks:
-        for g in ((256, 512) if quick else (32, 64, 128, 256, 512)):
+        for g in ((512, 1024) if quick else (32, 64, 128, 256, 512, 1024)):
             for block, sync in (shapes if not quick else [(256, True), (512, True)]):
                 out.append(WalkConfig("group", g, block, sync))
         out.append(WalkConfig("group", 256, 256, True, regcap=80))

@@ -150,6 +150,27 @@ def test_reference_init_interface(backend, lx, oracle):
         assert (keys[t] == walked).all(), t
 
 
+def test_reference_init_interface_at_group_1024(lx, oracle):
+    """The largest group (its table in constant memory): Backend::init from
+    u(k-8), u(k) gives the oracle's keys, as the ladder start does."""
+    lanes = 256
+    with lx.Backend(device=0, lanes=lanes, batch=1024) as b:
+        setup = lx.seeded_setup(212, lanes)
+        upc = np.zeros((lanes, 16), np.uint32)
+        for t in range(lanes):
+            k = bytes(setup.scalars[t])
+            upc[t, :8] = np.frombuffer(oracle.x25519_base(oracle.previous_scalar(k)), "<u4")
+            upc[t, 8:] = np.frombuffer(oracle.x25519_base(k), "<u4")
+        b.init(upc)
+        _, dump_a, _, _ = _walk(b, lx, setup, "b0", 1, dump_lanes=4, dump_keys=1024)
+        b.init_from_scalars(setup.scalars)
+        _, dump_b, _, _ = _walk(b, lx, setup, "b0", 1, dump_lanes=4, dump_keys=1024)
+    assert (dump_a == dump_b).all()
+    keys = _keys_of(dump_a, 4, 1024)
+    for t in range(4):
+        assert (keys[t] == oracle.walk_keys(bytes(setup.scalars[t]), 1024)).all(), t
+
+
 def test_hits_match_oracle_search(backend, lx, oracle):
     """Every hit of a 2-nibble search over 4096 lanes x 256 keys, exactly."""
     lanes = backend.threads()
@@ -233,7 +254,7 @@ def test_other_aspects(backend, lx, oracle, aspect):
 
 @pytest.mark.parametrize("walk,batch,block", [(1, 16, 256), (1, 32, 128), (1, 128, 256),
                                               (0, 32, 256), (0, 128, 128), (0, 256, 256),
-                                              (0, 512, 512), (0, 512, 256)])
+                                              (0, 512, 512), (0, 512, 256), (0, 1024, 512), (0, 1024, 128)])
 def test_other_batch_sizes(lx, oracle, walk, batch, block):
     with lx.Backend(device=0, lanes=512, batch=batch, block=block, walk=walk) as b:
         assert b.walk() == walk and b.batch() == batch
