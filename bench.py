@@ -434,7 +434,8 @@ def host_engine_main(a, world: int, rank: int) -> None:
                           "scaling": "weak", "engine": a.engine, "prefix": prefix, "ranks": ranks}), flush=True)
 
 
-def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_keys, steps, warmup, e2e=True) -> dict:
+def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_keys, steps, warmup, e2e=True,
+            shape: tuple[int, bool] | None = None) -> dict:
     """Times `steps` launches (after `warmup`) of the walk over `total_keys`
     keys in all, device-timed with CUDA events on the launching stream; every
     hit is rechecked from scratch on the CPU."""
@@ -442,10 +443,13 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
     # A stream of our own (never the legacy default stream, whose handle is 0):
     # the library launches on it and the timing events are recorded on it.
     stream = torch.cuda.Stream(device=dev)
-    with lx.Backend(device=dev, lanes=0, batch=batch, block=a.block, walk=walk_id) as b0:
+    # Launch shape: --block (0: the library's default), or the section's own (threads per block, phase barrier).
+    block, flags = (shape[0], lx.FLAG_PHASE_SYNC if shape[1] else 0) if shape else (a.block, 0)
+    with lx.Backend(device=dev, lanes=0, batch=batch, block=block, walk=walk_id, flags=flags) as b0:
         wave = b0.threads()
     lanes = a.lanes or wave * max(1, -(-131072 // wave))
-    b = lx.Backend(device=dev, lanes=lanes, batch=batch, block=a.block, walk=walk_id, stream=stream.cuda_stream)
+    b = lx.Backend(device=dev, lanes=lanes, batch=batch, block=block, walk=walk_id, flags=flags,
+                   stream=stream.cuda_stream)
     setup = lx.seeded_setup(replicas.rank_seed(SEED, rank), lanes)
     t0 = time.perf_counter()
     b.init_from_scalars(setup.scalars)
@@ -533,6 +537,7 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
         roofline = dict(imad_line, bound="imad", traffic=None, alu_peak=alu_peak / 1e12)
     config = {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, seeded walkers, 2^36 keys per run)",
               "walk": walk, "prefix": prefix, "lanes_per_gpu": lanes, "batch": batch, "iters_per_step": iters,
+              "block": block or 512, "phase_barrier": bool(flags) if block else True,
               "keys_per_step_per_gpu": keys_per_step, "parallelism": f"replicas x{world}",
               "l2": "working set (lane state + per-lane batch buffers) exceeds L2; no flush needed"}
     rank_record = {"rank": rank, "device": dev, "seed": replicas.rank_seed(SEED, rank), "ms": ms_rank,
