@@ -492,7 +492,6 @@ int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args) {
     lxk::EmitArgs em;
     memset(&em, 0, sizeof em);
     fill_addr_consts(em.ac, args->ed, args->name_hash, args->want, args->mask);
-    lxsha::fold_chain(em.ac.ed, em.cc);
     if (int rc = ensure_hits(h, std::max<uint32_t>(args->max_hits, 1))) return rc;
     em.hit_count = h->d_hit_count;
     em.hits = h->d_hits;

@@ -40,7 +40,6 @@ namespace lxk {
 
 struct PoolSearch {
     lxsha::AddrConsts ac;
-    lxsha::ChainConsts cc;  // lxsha::fold_chain of ac.ed
 };
 
 struct PoolHit {
@@ -71,7 +70,7 @@ struct PoolArgs {
 };
 
 struct PoolEmit {
-    const PoolSearch& ps;          // shared memory: this warp's search
+    const lxsha::AddrConsts& ac;   // shared memory: this warp's search
     uint32_t* hit_count;
     PoolHit* hits;
     uint32_t max_hits;
@@ -81,8 +80,7 @@ struct PoolEmit {
     uint32_t one;  // from the kernel parameters
     __device__ __forceinline__ void operator()(const fe& u, uint64_t key) const {
         uint32_t d[4];
-        const lxsha::AddrConsts& ac = ps.ac;
-        lxsha::dest_hash_folded(u.v, ps.cc, ac.nh, one, d);
+        lxsha::dest_hash_one(u.v, ac.ed, ac, one, d);
         const bool match = ((d[0] & ac.mask[0]) == ac.want[0]) & ((d[1] & ac.mask[1]) == ac.want[1]) &
                            ((d[2] & ac.mask[2]) == ac.want[2]) & ((d[3] & ac.mask[3]) == ac.want[3]);
         if (active && match) {
@@ -99,7 +97,7 @@ struct PoolEmit {
 template <int M>
 static __global__ void __launch_bounds__(32 * kPoolWarps, 1) pool_walk_kernel(const __grid_constant__ PoolArgs<M> a) {
     __shared__ uint32_t s_item;
-    __shared__ PoolSearch s_ps[kPoolWarps];
+    __shared__ lxsha::AddrConsts s_ac[kPoolWarps];
     const uint32_t warp = threadIdx.x >> 5, lid = threadIdx.x & 31;
     const uint32_t nq = *a.n_queue;
     const uint32_t n_items = (nq + kPoolWarps - 1) / kPoolWarps;
@@ -112,22 +110,22 @@ static __global__ void __launch_bounds__(32 * kPoolWarps, 1) pool_walk_kernel(co
         const bool active = qi < nq;  // a short last item: spare warps walk a copy and write nothing
         const uint32_t chunk = a.queue[active ? qi : nq - 1];
         const uint32_t search = a.chunk_search[chunk];
-        constexpr int kWords = sizeof(PoolSearch) / 4;
-        for (int k = lid; k < kWords; k += 32)
-            reinterpret_cast<uint32_t*>(&s_ps[warp])[k] = reinterpret_cast<const uint32_t*>(&a.searches[search])[k];
+        constexpr int kWords = sizeof(lxsha::AddrConsts) / 4;
+        if (lid < kWords)
+            reinterpret_cast<uint32_t*>(&s_ac[warp])[lid] = reinterpret_cast<const uint32_t*>(&a.searches[search].ac)[lid];
         __syncwarp();
         const uint32_t lane = chunk * 32 + lid;
         fe uc = load_fe(a.state, 0, lane, a.capacity);
         fe vc = load_fe(a.state, 1, lane, a.capacity);
         uint64_t n = a.ns[lane];
-        const PoolEmit emit{s_ps[warp], a.hit_count, a.hits, a.max_hits, search, a.chunk_first[chunk] + lid, active, a.one};
+        const PoolEmit emit{s_ac[warp], a.hit_count, a.hits, a.max_hits, search, a.chunk_first[chunk] + lid, active, a.one};
         walk_groups<M, true>(uc, vc, n, a.groups, a.t, emit);
         if (active) {
             store_fe(a.state, 0, lane, a.capacity, uc);
             store_fe(a.state, 1, lane, a.capacity, vc);
             a.ns[lane] = n;
         }
-        __syncthreads();  // s_item and s_ps are rewritten next
+        __syncthreads();  // s_item and s_ac are rewritten next
     }
 }
 
@@ -483,7 +481,6 @@ static int pool_submit_body(lxmfv_pool* p, const lxmfv_search_desc* d, const uin
     memcpy(ps.ac.nh, d->name_hash, sizeof ps.ac.nh);
     memcpy(ps.ac.want, d->want, sizeof ps.ac.want);
     memcpy(ps.ac.mask, d->mask, sizeof ps.ac.mask);
-    lxsha::fold_chain(ps.ac.ed, ps.cc);
     cudaError_t e = cudaMemcpyAsync(&p->d_searches[slot], &ps, sizeof ps, cudaMemcpyHostToDevice, p->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->d_scalars, scalars, (size_t)d->lanes * 32, cudaMemcpyHostToDevice, p->stream);
     if (e == cudaSuccess)

@@ -41,7 +41,6 @@ struct Hit {
 // What a finished key is checked against and where results go.
 struct EmitArgs {
     lxsha::AddrConsts ac;
-    lxsha::ChainConsts cc;  // the search's folded chain constants (lxsha::fold_chain of ac.ed)
     uint32_t* hit_count;
     Hit* hits;
     uint32_t max_hits;
@@ -79,7 +78,7 @@ __device__ __forceinline__ void store_fe(uint32_t* st, int e, uint32_t lane, uin
 template <bool DUMP>
 __device__ __forceinline__ void emit_key(const EmitArgs& a, uint32_t lane, uint64_t key, uint64_t key0, const fe& u) {
     uint32_t d[4];
-    lxsha::dest_hash_folded(u.v, a.cc, a.ac.nh, a.ac.one, d);
+    lxsha::dest_hash(u.v, a.ac.ed, a.ac, d);
     const bool match = ((d[0] & a.ac.mask[0]) == a.ac.want[0]) & ((d[1] & a.ac.mask[1]) == a.ac.want[1]) &
                        ((d[2] & a.ac.mask[2]) == a.ac.want[2]) & ((d[3] & a.ac.mask[3]) == a.ac.want[3]);
     if (match) {
