@@ -20,8 +20,7 @@ struct __align__(16) fe {
 // reached by a call.  Measured on B200 against the bodies inlined at every
 // call site: the grouped walk +1.5% and the pool kernel +2% (smaller loops for
 // the instruction caches), the x-only walk -2.3% (four times the multiplies
-// per key, so the calls cost more than the code size saves); the x-only walk
-// therefore uses fe_mul_inl / fe_sqr_inl below.
+// per key, so the calls cost more than the code size saves).
 static __device__ __noinline__ fe fe_mul(const fe& a, const fe& b) {
     fe o;
     fe_mul_ptx(o, a, b);
@@ -29,21 +28,6 @@ static __device__ __noinline__ fe fe_mul(const fe& a, const fe& b) {
 }
 
 static __device__ __noinline__ fe fe_sqr(const fe& a) {
-    fe o;
-    fe_sqr_ptx(o, a);
-    return o;
-}
-
-// The same bodies inlined at the call site, for the x-only walk: it makes
-// four times the multiplies per key of the grouped walk, and its calls cost it
-// more than the larger loop does.
-__device__ __forceinline__ fe fe_mul_inl(const fe& a, const fe& b) {
-    fe o;
-    fe_mul_ptx(o, a, b);
-    return o;
-}
-
-__device__ __forceinline__ fe fe_sqr_inl(const fe& a) {
     fe o;
     fe_sqr_ptx(o, a);
     return o;
@@ -186,57 +170,39 @@ __device__ __forceinline__ fe fe_mul_small(const fe& a, uint32_t k) {
 
 // The canonical representative in [0, p): fold bit 255 (2^255 = 19), which
 // leaves x < 2^255 + 19 < 2p, then subtract p once when x + 19 reaches 2^255.
-// Both steps are rare branches around their long form: the fold carries out
-// of limb 0 only when limb 0 is within 19 of 2^32 (about 2^-28 of inputs),
-// and x can reach p only when its top limb is 0x7fffffff or more (about
-// 2^-31), so the common case is one add, two tests and no selects.
 __device__ __forceinline__ fe fe_canon(const fe& a) {
     fe o;
     asm("{\n\t"
-        ".reg .u32 t, c, y0, y1, y2, y3, y4, y5, y6, y7, m;\n\t"
-        ".reg .pred p;\n\t"
+        ".reg .u32 t, x0, x1, x2, x3, x4, x5, x6, x7, y0, y1, y2, y3, y4, y5, y6, y7, m;\n\t"
         "shr.u32 t, %15, 31;\n\t"
-        "and.b32 %7, %15, 0x7fffffff;\n\t"
+        "and.b32 x7, %15, 0x7fffffff;\n\t"
         "mul.lo.u32 t, t, 19;\n\t"
-        "mov.u32 %1, %9;\n\t"
-        "mov.u32 %2, %10;\n\t"
-        "mov.u32 %3, %11;\n\t"
-        "mov.u32 %4, %12;\n\t"
-        "mov.u32 %5, %13;\n\t"
-        "mov.u32 %6, %14;\n\t"
-        "add.cc.u32 %0, %8, t;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "setp.eq.u32 p, c, 0;\n\t"
-        "@p bra CFOLDED;\n\t"
-        "add.cc.u32 %1, %1, 1;\n\t"
-        "addc.cc.u32 %2, %2, 0;\n\t"
-        "addc.cc.u32 %3, %3, 0;\n\t"
-        "addc.cc.u32 %4, %4, 0;\n\t"
-        "addc.cc.u32 %5, %5, 0;\n\t"
-        "addc.cc.u32 %6, %6, 0;\n\t"
-        "addc.u32 %7, %7, 0;\n\t"
-        "CFOLDED:\n\t"
-        "setp.lt.u32 p, %7, 0x7fffffff;\n\t"
-        "@p bra CANONED;\n\t"
-        "add.cc.u32 y0, %0, 19;\n\t"
-        "addc.cc.u32 y1, %1, 0;\n\t"
-        "addc.cc.u32 y2, %2, 0;\n\t"
-        "addc.cc.u32 y3, %3, 0;\n\t"
-        "addc.cc.u32 y4, %4, 0;\n\t"
-        "addc.cc.u32 y5, %5, 0;\n\t"
-        "addc.cc.u32 y6, %6, 0;\n\t"
-        "addc.u32 y7, %7, 0;\n\t"
+        "add.cc.u32 x0, %8, t;\n\t"
+        "addc.cc.u32 x1, %9, 0;\n\t"
+        "addc.cc.u32 x2, %10, 0;\n\t"
+        "addc.cc.u32 x3, %11, 0;\n\t"
+        "addc.cc.u32 x4, %12, 0;\n\t"
+        "addc.cc.u32 x5, %13, 0;\n\t"
+        "addc.cc.u32 x6, %14, 0;\n\t"
+        "addc.u32 x7, x7, 0;\n\t"
+        "add.cc.u32 y0, x0, 19;\n\t"
+        "addc.cc.u32 y1, x1, 0;\n\t"
+        "addc.cc.u32 y2, x2, 0;\n\t"
+        "addc.cc.u32 y3, x3, 0;\n\t"
+        "addc.cc.u32 y4, x4, 0;\n\t"
+        "addc.cc.u32 y5, x5, 0;\n\t"
+        "addc.cc.u32 y6, x6, 0;\n\t"
+        "addc.u32 y7, x7, 0;\n\t"
         "shr.s32 m, y7, 31;\n\t"
         "and.b32 y7, y7, 0x7fffffff;\n\t"
-        "xor.b32 t, %0, y0;\n\t and.b32 t, t, m;\n\t xor.b32 %0, %0, t;\n\t"
-        "xor.b32 t, %1, y1;\n\t and.b32 t, t, m;\n\t xor.b32 %1, %1, t;\n\t"
-        "xor.b32 t, %2, y2;\n\t and.b32 t, t, m;\n\t xor.b32 %2, %2, t;\n\t"
-        "xor.b32 t, %3, y3;\n\t and.b32 t, t, m;\n\t xor.b32 %3, %3, t;\n\t"
-        "xor.b32 t, %4, y4;\n\t and.b32 t, t, m;\n\t xor.b32 %4, %4, t;\n\t"
-        "xor.b32 t, %5, y5;\n\t and.b32 t, t, m;\n\t xor.b32 %5, %5, t;\n\t"
-        "xor.b32 t, %6, y6;\n\t and.b32 t, t, m;\n\t xor.b32 %6, %6, t;\n\t"
-        "xor.b32 t, %7, y7;\n\t and.b32 t, t, m;\n\t xor.b32 %7, %7, t;\n\t"
-        "CANONED:\n\t"
+        "xor.b32 t, x0, y0;\n\t and.b32 t, t, m;\n\t xor.b32 %0, x0, t;\n\t"
+        "xor.b32 t, x1, y1;\n\t and.b32 t, t, m;\n\t xor.b32 %1, x1, t;\n\t"
+        "xor.b32 t, x2, y2;\n\t and.b32 t, t, m;\n\t xor.b32 %2, x2, t;\n\t"
+        "xor.b32 t, x3, y3;\n\t and.b32 t, t, m;\n\t xor.b32 %3, x3, t;\n\t"
+        "xor.b32 t, x4, y4;\n\t and.b32 t, t, m;\n\t xor.b32 %4, x4, t;\n\t"
+        "xor.b32 t, x5, y5;\n\t and.b32 t, t, m;\n\t xor.b32 %5, x5, t;\n\t"
+        "xor.b32 t, x6, y6;\n\t and.b32 t, t, m;\n\t xor.b32 %6, x6, t;\n\t"
+        "xor.b32 t, x7, y7;\n\t and.b32 t, t, m;\n\t xor.b32 %7, x7, t;\n\t"
         "}"
         : "=r"(o.v[0]), "=r"(o.v[1]), "=r"(o.v[2]), "=r"(o.v[3]), "=r"(o.v[4]), "=r"(o.v[5]), "=r"(o.v[6]),
           "=r"(o.v[7])

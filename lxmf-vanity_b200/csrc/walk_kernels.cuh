@@ -127,13 +127,13 @@ static __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_c
         fe acc = fe_one();
 #pragma unroll 1
         for (int i = 0; i < B; ++i) {
-            ys[i] = fe_mul_inl(xc, acc);
+            ys[i] = fe_mul(xc, acc);
             zs[i] = zc;
-            acc = fe_mul_inl(acc, zc);
-            const fe t1 = fe_sub(fe_mul_inl(xc, a.q), zc);
-            const fe t2 = fe_sub(xc, fe_mul_inl(zc, a.q));
-            const fe xn = fe_mul_inl(zp, fe_sqr_inl(t1));
-            const fe zn = fe_mul_inl(xp, fe_sqr_inl(t2));
+            acc = fe_mul(acc, zc);
+            const fe t1 = fe_sub(fe_mul(xc, a.q), zc);
+            const fe t2 = fe_sub(xc, fe_mul(zc, a.q));
+            const fe xn = fe_mul(zp, fe_sqr(t1));
+            const fe zn = fe_mul(xp, fe_sqr(t2));
             xp = xc;
             zp = zc;
             xc = xn;
@@ -142,8 +142,8 @@ static __global__ void __launch_bounds__(BLOCK, MINB) walk_kernel(const __grid_c
         fe inv = fe_invert(acc);
 #pragma unroll 1
         for (int i = B - 1; i >= 0; --i) {
-            const fe u = fe_canon(fe_mul_inl(ys[i], inv));
-            inv = fe_mul_inl(inv, zs[i]);
+            const fe u = fe_canon(fe_mul(ys[i], inv));
+            inv = fe_mul(inv, zs[i]);
             if (active) emit_key<DUMP>(a.em, lane, n + (uint64_t)i, key0, u);
         }
         n += B;
