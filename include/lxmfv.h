@@ -217,6 +217,19 @@ int lxmfv_pool_info(const lxmfv_pool* p, lxmfv_pool_info_t* info);
  * no free slot (admission against the memory budget). */
 int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* desc, const uint8_t* scalars, uint32_t* search_id);
 
+/* Admits searches descs[0..n) in order, as many as fit: the longest prefix
+ * for which the pool has free lanes and slots.  `scalars` holds every
+ * search's start scalars back to back (descs[0].lanes of them, then
+ * descs[1].lanes, ...).  Their start points run in one kernel, enqueued on
+ * the pool's stream without waiting (lxmfv_pool_submit waits for each), so a
+ * serving loop admits everything that arrived during a step at the cost of
+ * one launch; the next step runs after it.  search_ids[i] receives the id of
+ * descs[i] for i < *n_admitted.  LXMFV_ERR_OVERFLOW (nothing admitted) when
+ * descs[0] does not fit; a CUDA error of the start kernel itself shows at the
+ * next lxmfv_pool_poll. */
+int lxmfv_pool_submit_many(lxmfv_pool* p, const lxmfv_search_desc* descs, uint32_t n, const uint8_t* scalars,
+                           uint32_t* search_ids, uint32_t* n_admitted);
+
 /* Frees a search's lanes; it takes no further part in steps. */
 int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id);
 

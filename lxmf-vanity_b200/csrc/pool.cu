@@ -508,6 +508,110 @@ static int pool_submit_body(lxmfv_pool* p, const lxmfv_search_desc* d, const uin
     return LXMFV_OK;
 }
 
+// Admission of many searches with one start kernel and no host wait.  The
+// staging buffers (d_scalars, d_lane_map) are rewritten only by later copies on
+// the same stream, so they are never overwritten before this kernel has read
+// them, and every host source is copied out before its cudaMemcpyAsync
+// returns (pageable memory).
+static int pool_submit_many_body(lxmfv_pool* p, const lxmfv_search_desc* descs, uint32_t n, const uint8_t* scalars,
+                                 uint32_t* search_ids, uint32_t* n_admitted) {
+    if (!p || !n_admitted || (n && (!descs || !scalars || !search_ids))) return pfail(p, LXMFV_ERR_ARG, "null argument");
+    *n_admitted = 0;
+    if (n == 0) return LXMFV_OK;
+    // How many fit, in order; every admitted search's descriptor and scalars are checked first.
+    uint64_t free_lanes = (uint64_t)p->free_chunks.size() * 32, lanes_total = 0;
+    uint32_t free_slots = 0;
+    for (const auto& s : p->searches) free_slots += s.active ? 0 : 1;
+    uint32_t take = 0;
+    size_t off = 0;
+    for (; take < n; take++) {
+        const lxmfv_search_desc& d = descs[take];
+        if (d.lanes == 0 || d.lanes % 32)
+            return pfail(p, LXMFV_ERR_ARG, "search %u: lanes %u, a positive multiple of 32", take, d.lanes);
+        if (lanes_total + d.lanes > free_lanes || take >= free_slots) break;
+        for (uint32_t t = 0; t < d.lanes; t++) {
+            const uint8_t* k = scalars + off + 32 * (size_t)t;
+            if ((k[0] & 7) != 0 || (k[31] & 0xC0) != 0x40)
+                return pfail(p, LXMFV_ERR_ARG, "search %u: scalar %u is not clamped", take, t);
+        }
+        lanes_total += d.lanes;
+        off += 32 * (size_t)d.lanes;
+    }
+    if (take == 0)
+        return pfail(p, LXMFV_ERR_OVERFLOW, "%u lanes asked, %llu free, %u slots free", descs[0].lanes,
+                     (unsigned long long)free_lanes, free_slots);
+    PCU(p, cudaSetDevice(p->device));
+    std::vector<uint32_t> lane_map(lanes_total);
+    std::vector<uint32_t> slots(take);
+    uint32_t slot = 0;
+    size_t at = 0;
+    cudaError_t e = cudaSuccess;
+    uint32_t done = 0;
+    for (; done < take; done++) {
+        const lxmfv_search_desc& d = descs[done];
+        while (p->searches[slot].active) slot++;  // a free slot exists: counted above
+        auto& s = p->searches[slot];
+        s.chunks.clear();
+        for (uint32_t i = 0; i < d.lanes / 32; i++) {
+            s.chunks.push_back(p->free_chunks.back());
+            p->free_chunks.pop_back();
+        }
+        std::sort(s.chunks.begin(), s.chunks.end());
+        for (uint32_t i = 0; i < d.lanes / 32; i++) {
+            const uint32_t c = s.chunks[i];
+            p->chunk_owner[c] = (int32_t)slot;
+            p->h_chunk_search[c] = slot;
+            p->h_chunk_first[c] = 32 * i;
+            for (uint32_t j = 0; j < 32; j++) lane_map[at + 32 * i + j] = 32 * c + j;
+        }
+        at += d.lanes;
+        s.active = true;  // claimed, so the next search takes another slot
+        s.lanes = d.lanes;
+        s.keys_per_lane = 0;
+        slots[done] = slot;
+        lxk::PoolSearch ps;
+        memset(&ps, 0, sizeof ps);
+        ps.ac.one = 1;
+        memcpy(ps.ac.ed, d.ed, sizeof ps.ac.ed);
+        memcpy(ps.ac.nh, d.name_hash, sizeof ps.ac.nh);
+        memcpy(ps.ac.want, d.want, sizeof ps.ac.want);
+        memcpy(ps.ac.mask, d.mask, sizeof ps.ac.mask);
+        e = cudaMemcpyAsync(&p->d_searches[slot], &ps, sizeof ps, cudaMemcpyHostToDevice, p->stream);
+        if (e != cudaSuccess) {
+            done++;
+            break;
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p->d_scalars, scalars, 32 * (size_t)lanes_total, cudaMemcpyHostToDevice, p->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p->d_lane_map, lane_map.data(), sizeof(uint32_t) * lanes_total, cudaMemcpyHostToDevice,
+                            p->stream);
+    if (e == cudaSuccess) {
+        lxk::pool_start_kernel<<<(unsigned)((lanes_total + 127) / 128), 128, 0, p->stream>>>(
+            p->d_state, p->d_ns, p->capacity, p->d_scalars, p->d_lane_map, (uint32_t)lanes_total, p->m, pool_u8b(),
+            pool_v8b());
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        for (uint32_t i = 0; i < done; i++) {
+            auto& s = p->searches[slots[i]];
+            for (uint32_t c : s.chunks) {
+                p->chunk_owner[c] = -1;
+                p->free_chunks.push_back(c);
+            }
+            s.chunks.clear();
+            s.active = false;
+            s.lanes = 0;
+        }
+        return pfail(p, LXMFV_ERR_CUDA, "submit: %s", cudaGetErrorString(e));
+    }
+    for (uint32_t i = 0; i < take; i++) search_ids[i] = slots[i];
+    *n_admitted = take;
+    p->queue_dirty = true;
+    p->err.clear();
+    return LXMFV_OK;
+}
+
 static int pool_retire_body(lxmfv_pool* p, uint32_t search_id) {
     if (!p) return LXMFV_ERR_ARG;
     if (search_id >= p->max_searches || !p->searches[search_id].active)
@@ -582,6 +686,11 @@ int lxmfv_pool_open(const lxmfv_pool_options* opts, lxmfv_pool** out) {
 
 int lxmfv_pool_submit(lxmfv_pool* p, const lxmfv_search_desc* d, const uint8_t* scalars, uint32_t* search_id) {
     return no_throw(&p, [&] { return pool_submit_body(p, d, scalars, search_id); });
+}
+
+int lxmfv_pool_submit_many(lxmfv_pool* p, const lxmfv_search_desc* descs, uint32_t n, const uint8_t* scalars,
+                           uint32_t* search_ids, uint32_t* n_admitted) {
+    return no_throw(&p, [&] { return pool_submit_many_body(p, descs, n, scalars, search_ids, n_admitted); });
 }
 
 int lxmfv_pool_retire(lxmfv_pool* p, uint32_t search_id) {

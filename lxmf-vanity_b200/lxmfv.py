@@ -121,6 +121,7 @@ SIGNATURES = {
     "lxmfv_pool_last_error": ([C.c_void_p], C.c_char_p),
     "lxmfv_pool_info": ([C.c_void_p, C.POINTER(PoolInfo)], C.c_int),
     "lxmfv_pool_submit": ([C.c_void_p, C.POINTER(SearchDesc), _u8p, _u32p], C.c_int),
+    "lxmfv_pool_submit_many": ([C.c_void_p, C.POINTER(SearchDesc), C.c_uint32, _u8p, _u32p, _u32p], C.c_int),
     "lxmfv_pool_retire": ([C.c_void_p, C.c_uint32], C.c_int),
     "lxmfv_pool_step": ([C.c_void_p, C.c_uint32], C.c_int),
     "lxmfv_pool_poll": ([C.c_void_p, C.POINTER(PoolHit), C.c_uint32, _u32p], C.c_int),

@@ -137,6 +137,23 @@ class Pool:
         self.specs[sid.value] = spec
         return sid.value
 
+    def submit_many(self, specs: list[SearchSpec]) -> list[int]:
+        """Admits the longest prefix of `specs` that fits (lxmfv_pool_submit_many:
+        one start kernel for all, no wait); returns their ids.  Raises
+        LxmfvError (ERR_OVERFLOW) when the first does not fit."""
+        if not specs:
+            return []
+        descs = (lx.SearchDesc * len(specs))(*[sp.desc() for sp in specs])
+        scal = np.ascontiguousarray(np.concatenate([sp.scalars for sp in specs]), np.uint8)
+        ids = (C.c_uint32 * len(specs))()
+        got = C.c_uint32()
+        self._check(lx.lib().lxmfv_pool_submit_many(self._h, descs, len(specs),
+                                                    scal.ctypes.data_as(C.POINTER(C.c_uint8)), ids, C.byref(got)))
+        out = [ids[i] for i in range(got.value)]
+        for sid, sp in zip(out, specs):
+            self.specs[sid] = sp
+        return out
+
     def retire(self, sid: int) -> None:
         self._check(lx.lib().lxmfv_pool_retire(self._h, sid))
         self.specs.pop(sid, None)
@@ -300,8 +317,10 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
         while pending and pending[0].arrival <= now:
             waiting.append(pending.popleft())
         while waiting:
+            # Everything that arrived and fits, in arrival order, in one
+            # admission (one start kernel, queued ahead of the next step).
             try:
-                sid = pool.submit(waiting[0].spec)
+                sids = pool.submit_many([r.spec for r in waiting])
             except lx.LxmfvError as e:
                 if e.code != lx.ERR_OVERFLOW:
                     raise
@@ -313,9 +332,13 @@ def serve(pool: Pool, requests: list[Request], groups: int = 1, time_limit: floa
                 r.done = time.perf_counter() - t0
                 failed.append(r)
                 continue
-            r = waiting.popleft()
-            r.admitted = time.perf_counter() - t0
-            active[sid] = r
+            t_adm = time.perf_counter() - t0
+            for sid in sids:
+                r = waiting.popleft()
+                r.admitted = t_adm
+                active[sid] = r
+            if waiting and active:
+                break  # the rest wait for lanes
         if not active:
             if pending:
                 time.sleep(max(0.0, min(pending[0].arrival - now, 0.05)))

@@ -40,6 +40,17 @@ class HostPool:
         self.max_active = max(self.max_active, len(self.active))
         return sid
 
+    def submit_many(self, specs: list) -> list:
+        """lxmfv_pool_submit_many: the longest prefix that fits; overflow when the first does not."""
+        ids = []
+        for spec in specs:
+            if self.used + spec.lanes > self.capacity:
+                break
+            ids.append(self.submit(spec))
+        if not ids:
+            raise lx.LxmfvError(lx.ERR_OVERFLOW, "no lanes free")
+        return ids
+
     def step(self, groups: int = 1) -> None:
         for sid in self.active:
             self.walked[sid] += self.batch * groups
