@@ -180,7 +180,7 @@ typedef struct {
     int32_t device;
     uint32_t capacity_lanes; /* walker lanes in the pool; 0: memory_budget / bytes per lane, else 2^20 */
     uint64_t memory_budget;  /* device bytes for lanes (108 per lane) when capacity_lanes is 0 */
-    uint32_t batch;          /* keys per group: 64, 128, 256 or 512; 0: 512 */
+    uint32_t batch;          /* keys per group: 64, 128, 256, 512 or 1024; 0: 512 */
     uint32_t max_searches;   /* search slots; 0: 4096 */
     uint32_t max_hits;       /* hits held between polls; 0: 65536 */
     void* stream;            /* cudaStream_t; NULL: a stream of the pool's own */

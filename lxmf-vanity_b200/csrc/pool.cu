@@ -50,6 +50,15 @@ struct PoolHit {
 
 constexpr int kPoolWarps = 16;  // warps per block (512 threads)
 
+// The pool's group table: in the parameters up to M = 256, in constant
+// memory (c_group_u / c_group_v, written at lxmfv_pool_open) at M = 512.
+struct NoTable {};
+template <int M>
+using PoolTableFor = typename std::conditional<(M > 256), NoTable, GroupTable<M>>::type;
+template <int M>
+__device__ __forceinline__ const GroupTable<M>& pool_table(const GroupTable<M>& t) { return t; }
+__device__ __forceinline__ ConstGroupTable pool_table(const NoTable&) { return ConstGroupTable{}; }
+
 template <int M>
 struct PoolArgs {
     uint32_t* state;               // [16][capacity]: u_C, v_C
@@ -66,7 +75,7 @@ struct PoolArgs {
     PoolHit* hits;
     uint32_t max_hits;
     uint32_t one;                  // 1: the SHA-256 sums' multiplier (see madd)
-    GroupTable<M> t;
+    PoolTableFor<M> t;
 };
 
 struct PoolEmit {
@@ -119,7 +128,7 @@ static __global__ void __launch_bounds__(32 * kPoolWarps, 1) pool_walk_kernel(co
         fe vc = load_fe(a.state, 1, lane, a.capacity);
         uint64_t n = a.ns[lane];
         const PoolEmit emit{s_ac[warp], a.hit_count, a.hits, a.max_hits, search, a.chunk_first[chunk] + lid, active, a.one};
-        walk_groups<M, true>(uc, vc, n, a.groups, a.t, emit);
+        walk_groups<M, true>(uc, vc, n, a.groups, pool_table(a.t), emit);
         if (active) {
             store_fe(a.state, 0, lane, a.capacity, uc);
             store_fe(a.state, 1, lane, a.capacity, vc);
@@ -238,6 +247,7 @@ const void* pool_kernel_for(uint32_t batch) {
         case 128: return pool_kernel_ptr<64>();
         case 256: return pool_kernel_ptr<128>();
         case 512: return pool_kernel_ptr<256>();
+        case 1024: return pool_kernel_ptr<512>();
     }
     return nullptr;
 }
@@ -259,9 +269,11 @@ void launch_pool(lxmfv_pool* p, uint32_t groups) {
     a.hits = p->d_hits;
     a.max_hits = p->max_hits;
     a.one = 1;
-    for (int i = 0; i <= M; i++) {
-        a.t.u[i] = p->tu[i];
-        a.t.v[i] = p->tv[i];
+    if constexpr (M <= 256) {
+        for (int i = 0; i <= M; i++) {
+            a.t.u[i] = p->tu[i];
+            a.t.v[i] = p->tv[i];
+        }
     }
     lxk::pool_walk_kernel<M><<<p->sms, 32 * lxk::kPoolWarps, 0, p->stream>>>(a);
 }
@@ -271,7 +283,8 @@ void launch_pool_any(lxmfv_pool* p, uint32_t groups) {
         case 64: launch_pool<32>(p, groups); break;
         case 128: launch_pool<64>(p, groups); break;
         case 256: launch_pool<128>(p, groups); break;
-        default: launch_pool<256>(p, groups); break;
+        case 512: launch_pool<256>(p, groups); break;
+        default: launch_pool<512>(p, groups); break;
     }
 }
 
@@ -347,7 +360,7 @@ static int pool_open_body(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     p->device = o.device;
     p->batch = o.batch ? o.batch : 512;  // 0: the autotuner's choice on the batched mix
     p->m = p->batch / 2;
-    if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128, 256 or 512", p->batch);
+    if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128, 256, 512 or 1024", p->batch);
     p->max_searches = o.max_searches ? o.max_searches : 4096;
     p->max_hits = o.max_hits ? o.max_hits : 65536;
     int count = 0;
@@ -422,6 +435,16 @@ static int pool_open_body(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
     cudaFree(du);
     cudaFree(dv);
+    if (e == cudaSuccess && p->m > 256) {
+        // Groups of 1024: the table goes to this module's constant memory (the
+        // same bytes for every pool on the device).
+        e = cudaMemcpyToSymbolAsync(lxk::c_group_u, p->tu, sizeof(fe) * (p->m + 1), 0, cudaMemcpyHostToDevice,
+                                    p->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyToSymbolAsync(lxk::c_group_v, p->tv, sizeof(fe) * (p->m + 1), 0, cudaMemcpyHostToDevice,
+                                        p->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+    }
     if (e != cudaSuccess) return pfail(p, LXMFV_ERR_CUDA, "pool table: %s", cudaGetErrorString(e));
     p->err.clear();
     return LXMFV_OK;

@@ -231,7 +231,8 @@ def run_batched(pool: Pool, specs: list[SearchSpec], steps: int, groups: int, wa
             "batch": pool.batch}
 
 
-def autotune(device: int, specs_fn, lanes_total: int, batches=(64, 128, 256, 512), groups=(1, 2, 4), steps: int = 3) -> dict:
+def autotune(device: int, specs_fn, lanes_total: int, batches=(64, 128, 256, 512, 1024), groups=(1, 2, 4),
+             steps: int = 3) -> dict:
     """Measures the pool's aggregate keys/s for each keys-per-group and step
     length on the given search mix; returns the fastest with all results."""
     results = []

@@ -28,7 +28,7 @@ def _oracle_hits(oracle, spec, keys):
     return out
 
 
-@pytest.mark.parametrize("batch", [64, 256, 512])
+@pytest.mark.parametrize("batch", [64, 256, 512, 1024])
 def test_pool_hits_match_oracle(srv, oracle, batch):
     specs = [srv.SearchSpec.seeded(11, "b0", "lxmf.delivery", 96),
              srv.SearchSpec.seeded(12, "7", "nomadnetwork.node", 64),
