@@ -5,7 +5,7 @@ Workload (the plain GPU search): one 8-hex-digit prefix (numpy-seeded),
 aspect lxmf.delivery, every lane starting from its own seeded clamped X25519
 scalar (ChaCha20 stream of the seed) with one shared Ed25519 key, 2^36 keys
 walked in total over the timed steps (a step is one launch that walks every
-lane `iters` groups further).  Keys per inversion: the tuned 512 for the
+lane `iters` groups further).  Keys per inversion: the tuned 1024 for the
 headline; the same 2^36 keys again at 64 (the reference kernel's BATCH), with
 the grouped walk (`at_batch_64`) and with the x-only walk, the reference's
 algorithm (`xadd_b64`).  Synthetic, seeded inputs; no dataset is involved.
@@ -43,7 +43,7 @@ sys.path.insert(0, os.path.join(ROOT, "lxmf-vanity_b200"))
 import lxmfv_replicas as replicas  # noqa: E402  (rank seeds, max over ranks)
 
 TOTAL_KEYS = 1 << 36
-BATCH = 512
+BATCH = 1024
 SEED = 3
 METRIC = "keys/s, plain GPU search (one 8-hex prefix, seeded walkers, 2^36 keys), bit-exact"
 
@@ -58,13 +58,18 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
     return (5 * m + 13) / b, (2 * m + 255) / b
 
 
-# Per key, from one ncu capture of each kernel (profiles/walk_group_g512_plain_search.md,
-# profiles/walk_group_g256_plain_search.md, profiles/walk_xadd_b128_plain_search.md):
-# ALU-pipe lane operations (the binding pipe), all instructions, and DRAM bytes (read + write).
+# Per key, from one ncu capture of each kernel (profiles/walk_group_g1024_plain_search.md,
+# profiles/walk_group_g64_plain_search.md, profiles/walk_xadd_b64_plain_search.md; the G = 512, 256 and x-only
+# B = 128 rows from the earlier captures in profiles/): ALU-pipe lane operations (the binding pipe: ALU pipe
+# active % x 64 lanes x SMs x clock / keys per second), all instructions (smsp__inst_executed x 32 / keys), and
+# DRAM bytes (read + write).
 NCU_PER_KEY = {
+    ("group", 1024): {"alu": 3221, "inst": 5764, "dram_bytes": 32.0},
     ("group", 512): {"alu": 3243, "inst": 5823, "dram_bytes": 31.6},
     ("group", 256): {"alu": 3288, "inst": 5935, "dram_bytes": 31.1},
+    ("group", 64): {"alu": 3556, "inst": 6605, "dram_bytes": 24.8},
     ("xadd", 128): {"alu": 4166, "inst": 8120, "dram_bytes": 131.9},
+    ("xadd", 64): {"alu": 4337, "inst": 8562, "dram_bytes": 132.1},
 }
 
 
@@ -82,7 +87,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--lanes", type=int, default=0, help="walker lanes per GPU (0: two full waves)")
-    p.add_argument("--batch", type=int, default=BATCH, help="keys per inversion (grouped walk: 32..512)")
+    p.add_argument("--batch", type=int, default=BATCH, help="keys per inversion (grouped walk: 32..1024)")
     p.add_argument("--walk", choices=["group", "xadd"], default="group")
     p.add_argument("--block", type=int, default=0)
     p.add_argument("--total-keys", type=float, default=float(TOTAL_KEYS))
@@ -265,12 +270,12 @@ def batched_workload(lx, dev: int, single_value: float) -> dict:
     """256 concurrent searches in the pool's persistent kernel: prefix lengths
     uniform over 4-10 nibbles with random hex, aspects uniform over three, each
     with its own seeded identity; 1184 lanes each, so that the persistent
-    kernel's work items (512 lanes) are exactly 4 per SM; G = 512, 4 groups per
+    kernel's work items (512 lanes) are exactly 4 per SM; G = 1024, 4 groups per
     step (the autotuned setting); aggregate device keys/s against the single
     search's `value`."""
     import lxmfv_serve as srv
     specs = srv.batched_specs(256, seed=4, lanes=1184, min_nibbles=4, max_nibbles=10)
-    with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=512) as pool:
+    with srv.Pool(device=dev, capacity_lanes=256 * 1184, batch=1024) as pool:
         r = srv.run_batched(pool, specs, steps=6, groups=4, warmup=1)  # every hit rechecked
     r["vs_single_search"] = r["keys_per_s"] / single_value
     r["workload"] = "256 searches, 4-10 nibbles, 3 aspects, 1184 lanes each, one persistent launch per step"

@@ -65,7 +65,7 @@ typedef struct lxmfv_handle lxmfv_handle;
 typedef struct {
     int32_t device;       /* CUDA device ordinal */
     uint32_t lanes;       /* walker lanes (GPU threads); 0: one full wave of the device */
-    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 1024; 0: the fastest (GROUP 512, XADD 128) */
+    uint32_t batch;       /* keys per inversion: XADD 16, 32, 64, 128; GROUP 32 .. 1024; 0: the fastest (GROUP 1024, XADD 128) */
     uint32_t block;       /* threads per block: 128, 256 or 512; 0: 512 with LXMFV_FLAG_PHASE_SYNC */
     uint32_t walk;        /* LXMFV_WALK_GROUP (0, default) or LXMFV_WALK_XADD */
     uint32_t flags;       /* LXMFV_FLAG_* */
@@ -180,7 +180,7 @@ typedef struct {
     int32_t device;
     uint32_t capacity_lanes; /* walker lanes in the pool; 0: memory_budget / bytes per lane, else 2^20 */
     uint64_t memory_budget;  /* device bytes for lanes (108 per lane) when capacity_lanes is 0 */
-    uint32_t batch;          /* keys per group: 64, 128, 256, 512 or 1024; 0: 512 */
+    uint32_t batch;          /* keys per group: 64, 128, 256, 512 or 1024; 0: 1024 */
     uint32_t max_searches;   /* search slots; 0: 4096 */
     uint32_t max_hits;       /* hits held between polls; 0: 65536 */
     void* stream;            /* cudaStream_t; NULL: a stream of the pool's own */

@@ -66,8 +66,8 @@ const char* USAGE =
     "                     the d-th GPU listed uses seed N + d, the CPU threads seed N + (number of\n"
     "                     GPUs); with --batch-file, search i of the file uses seed N + i\n"
     "  --walk group|xadd  the walk (default group; xadd is the x-only differential walk)\n"
-    "  --batch N          keys per inversion (default 512; --walk xadd: 128; with --batch-file, keys per\n"
-    "                     group: 512)\n"
+    "  --batch N          keys per inversion (default 1024; --walk xadd: 128; with --batch-file, keys per\n"
+    "                     group: 1024)\n"
     "  --lanes N          walker lanes per GPU (default: one full wave)";
 
 using Clock = std::chrono::steady_clock;
@@ -79,7 +79,7 @@ struct Options {
     std::vector<int> devices{0};
     bool seeded = false;
     uint64_t seed = 0;
-    uint32_t walk = LXMFV_WALK_GROUP, batch = 512, lanes = 0;
+    uint32_t walk = LXMFV_WALK_GROUP, batch = 0, lanes = 0;  // batch 0: the library's fastest
     bool batch_given = false;
     int threads = 0;  // CPU threads; 0: the mode's default
     std::string batch_file;
@@ -452,7 +452,7 @@ int run_batch_file(const Options& o) {
     const auto start = Clock::now();
     lxmfv_pool_options po{};
     po.device = o.devices[0];
-    po.batch = o.batch_given ? o.batch : 0;  // 0: the pool's default group of 512 keys
+    po.batch = o.batch_given ? o.batch : 0;  // 0: the pool's default group of 1024 keys
     po.max_searches = (uint32_t)std::min<size_t>(4096, searches.size());
     lxmfv_pool* pool = nullptr;
     int rc = lxmfv_pool_open(&po, &pool);

@@ -326,7 +326,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     h->device = o.device;
     h->walk = o.walk;
     // 0: the fastest keys per inversion of each walk (the autotuner's choice).
-    h->batch = o.batch ? o.batch : (o.walk == LXMFV_WALK_XADD ? 128 : 512);
+    h->batch = o.batch ? o.batch : (o.walk == LXMFV_WALK_XADD ? 128 : 1024);
     // Default launch shape (block 0): 512 threads with the phase barrier, the
     // fastest measured on B200 for both walks; otherwise the flags decide.
     h->block = o.block ? o.block : 512;

@@ -358,7 +358,7 @@ static int pool_open_body(const lxmfv_pool_options* opts, lxmfv_pool** out) {
     lxmfv_pool_options o{};
     if (opts) o = *opts;
     p->device = o.device;
-    p->batch = o.batch ? o.batch : 512;  // 0: the autotuner's choice on the batched mix
+    p->batch = o.batch ? o.batch : 1024;  // 0: the autotuner's choice on the batched mix
     p->m = p->batch / 2;
     if (!pool_kernel_for(p->batch)) return pfail(p, LXMFV_ERR_ARG, "batch %u: the pool walks groups of 64, 128, 256, 512 or 1024", p->batch);
     p->max_searches = o.max_searches ? o.max_searches : 4096;

@@ -86,7 +86,7 @@ class SearchSpec:
 class Pool:
     """The C ABI's search pool (lxmfv_pool_*)."""
 
-    def __init__(self, device: int = 0, capacity_lanes: int = 0, memory_budget: int = 0, batch: int = 512,
+    def __init__(self, device: int = 0, capacity_lanes: int = 0, memory_budget: int = 0, batch: int = 1024,
                  max_searches: int = 4096, max_hits: int = 65536, stream: int | None = None):
         L = lx.lib()
         o = lx.PoolOptions(device, capacity_lanes, memory_budget, batch, max_searches, max_hits, stream)

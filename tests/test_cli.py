@@ -178,8 +178,8 @@ def test_gpu_and_cpu_together(tmp_path):
 
 @pytest.mark.gpu
 def test_self_test_passes(tmp_path):
-    # 256 lanes x one batch of keys each: the default 512, and the reference's 64 (mod.rs:178-207).
-    for args, keys in (([], 256 * 512), (["--batch", "64"], 256 * 64)):
+    # 256 lanes x one batch of keys each: the default 1024, and the reference's 64 (mod.rs:178-207).
+    for args, keys in (([], 256 * 1024), (["--batch", "64"], 256 * 64)):
         r = run(["--gpu-self-test"] + args, tmp_path)
         assert r.returncode == 0, r.stderr
         m = re.search(r"Self-test passed: (\d+) public keys match X25519, (\d+) hits", r.stdout)
