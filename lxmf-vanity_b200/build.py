@@ -27,7 +27,8 @@ CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wextra"]
 
 CU_SOURCES = ["lxmfv.cu", "noalloc.cu", "pool.cu"]
 CXX_SOURCES = ["host.cpp", "cpu_search.cpp"]
-HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "prim_kernels.cuh",
+HEADERS = ["fe25519.cuh", "fe25519_ptx.cuh", "sha256_lxmf.cuh", "walk_kernels.cuh", "group_kernels.cuh", "ws_kernels.cuh",
+           "prim_kernels.cuh",
            "cpu_sha256.h"]
 
 

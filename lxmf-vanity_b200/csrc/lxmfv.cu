@@ -19,6 +19,7 @@
 #include "group_kernels.cuh"
 #include "prim_kernels.cuh"
 #include "walk_kernels.cuh"
+#include "ws_kernels.cuh"
 
 struct lxmfv_handle {
     int device = 0;
@@ -33,6 +34,8 @@ struct lxmfv_handle {
     uint32_t block = 256;
     bool sync = false;    // grouped walk: block barrier after each group
     bool low_regs = false;  // LXMFV_FLAG_REGCAP_80
+    bool ws = false;        // LXMFV_FLAG_WARP_SPEC: walker and hash warps
+    uint32_t* d_err = nullptr;  // set by a warp-specialised launch whose wait gave up
     uint32_t* d_state = nullptr;
     uint64_t* d_ns = nullptr;
     uint32_t* d_hit_count = nullptr;
@@ -117,6 +120,26 @@ const void* xadd_kernel_ptr(uint32_t block, bool sync, bool low_regs, bool dump)
     return dump ? xadd_kernel_ptr_d<B, true>(block, sync, low_regs) : xadd_kernel_ptr_d<B, false>(block, sync, low_regs);
 }
 
+// The warp-specialised grouped walk: 4 walker warps and 12 hash warps per
+// block (512 threads, 128 lanes), 6 slots per walker warp's ring.
+constexpr int kWsF = 4, kWsC = 3, kWsS = 6;
+constexpr uint32_t kWsLanesPerBlock = 32 * kWsF;
+constexpr size_t kWsSmem = sizeof(lxk::WsShared<kWsF, kWsS>);
+
+template <int M>
+const void* ws_kernel_ptr(bool dump) {
+    return dump ? (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, true>
+                : (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, false>;
+}
+
+const void* ws_kernel_for(uint32_t batch, bool dump) {
+    switch (batch) {
+        case 512: return ws_kernel_ptr<256>(dump);
+        case 1024: return ws_kernel_ptr<512>(dump);
+    }
+    return nullptr;
+}
+
 // The walk kernel of a configuration (null when unsupported).
 const void* walk_kernel_ptr(uint32_t walk, uint32_t batch, uint32_t block, bool sync, bool low_regs,
                             bool dump = false) {
@@ -146,6 +169,29 @@ void launch_xadd(lxmfv_handle* h, const lxk::WalkArgs& wa) {
     typedef void (*fn_t)(lxk::WalkArgs);
     const fn_t fn = (fn_t)xadd_kernel_ptr<B>(h->block, h->sync, h->low_regs, wa.em.dump_lanes > 0);
     fn<<<grid, h->block, 0, h->stream>>>(wa);
+}
+
+template <int M>
+void launch_group_ws(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
+    if constexpr (M == 256 || M == 512) {
+        lxk::WsArgs<M> a;
+        a.g.state = h->d_state;
+        a.g.ns = h->d_ns;
+        a.g.lanes = h->lanes;
+        a.g.iters = iters;
+        a.g.em = em;
+        if constexpr (M <= 256) {
+            for (int i = 0; i <= M; i++) {
+                a.g.t.u[i] = h->tu[i];
+                a.g.t.v[i] = h->tv[i];
+            }
+        }
+        a.err = h->d_err;
+        const unsigned grid = (h->lanes + kWsLanesPerBlock - 1) / kWsLanesPerBlock;
+        typedef void (*fn_t)(lxk::WsArgs<M>);
+        const fn_t fn = (fn_t)ws_kernel_ptr<M>(em.dump_lanes > 0);
+        fn<<<grid, 32 * kWsF * (1 + kWsC), kWsSmem, h->stream>>>(a);
+    }
 }
 
 template <int M>
@@ -184,6 +230,11 @@ void launch_walk(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters, const
             case 64: launch_xadd<64>(h, wa); break;
             default: launch_xadd<128>(h, wa); break;
         }
+    } else if (h->ws) {
+        if (h->batch == 512)
+            launch_group_ws<256>(h, em, iters);
+        else
+            launch_group_ws<512>(h, em, iters);
     } else {
         switch (h->batch) {
             case 32: launch_group<16>(h, em, iters); break;
@@ -332,6 +383,11 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     h->block = o.block ? o.block : 512;
     h->sync = o.block ? (o.flags & LXMFV_FLAG_PHASE_SYNC) != 0 : true;
     h->low_regs = (o.flags & LXMFV_FLAG_REGCAP_80) != 0;
+    h->ws = (o.flags & LXMFV_FLAG_WARP_SPEC) != 0;
+    if (h->ws && (h->walk != LXMFV_WALK_GROUP || !ws_kernel_for(h->batch, false) || h->low_regs ||
+                  (o.block && o.block != 512)))
+        return fail(h, LXMFV_ERR_ARG, "LXMFV_FLAG_WARP_SPEC needs the grouped walk, batch 512 or 1024 and block 0 or 512");
+    if (h->ws) h->block = 512;
     if (h->walk != LXMFV_WALK_GROUP && h->walk != LXMFV_WALK_XADD)
         return fail(h, LXMFV_ERR_ARG, "walk %u: 0 grouped, 1 x-only", h->walk);
     if (h->low_regs && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, true))
@@ -367,10 +423,24 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     CU(h, cudaEventCreate(&h->ev0));
     CU(h, cudaEventCreate(&h->ev1));
     int per_sm = 0;
-    CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs),
-                                                        (int)h->block, 0));
-    if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
-    h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;
+    if (h->ws) {
+        // The ring buffers take more than the default 48 KB of dynamic shared memory.
+        for (int dump = 0; dump < 2; dump++)
+            CU(h, cudaFuncSetAttribute(ws_kernel_for(h->batch, dump != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kWsSmem));
+        CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ws_kernel_for(h->batch, false), (int)h->block,
+                                                            kWsSmem));
+        if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "warp-specialised walk cannot be resident (batch %u)", h->batch);
+        h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * kWsLanesPerBlock;
+        CU(h, cudaMalloc(&h->d_err, sizeof(uint32_t)));
+        CU(h, cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), h->stream));
+    } else {
+        CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                  &per_sm, walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs), (int)h->block, 0));
+        if (per_sm < 1)
+            return fail(h, LXMFV_ERR_CUDA, "walk kernel cannot be resident (batch %u, block %u)", h->batch, h->block);
+        h->lanes = o.lanes ? o.lanes : (uint32_t)(h->sms * per_sm) * h->block;
+    }
     CU(h, cudaMalloc(&h->d_state, (size_t)h->lanes * 32 * sizeof(uint32_t)));
     CU(h, cudaMalloc(&h->d_ns, (size_t)h->lanes * sizeof(uint64_t)));
     CU(h, cudaMalloc(&h->d_hit_count, sizeof(uint32_t)));
@@ -535,8 +605,20 @@ int lxmfv_collect(lxmfv_handle* h, lxmfv_hit* hits, uint32_t hits_cap, uint32_t*
     if (dump_addr && dumped)
         CU(h, cudaMemcpy(dump_addr, h->d_dump_addr, dumped * 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     CU(h, cudaMemsetAsync(h->d_hit_count, 0, sizeof(uint32_t), h->stream));
+    uint32_t gave_up = 0;
+    if (h->d_err) {
+        CU(h, cudaMemcpy(&gave_up, h->d_err, sizeof gave_up, cudaMemcpyDeviceToHost));
+        CU(h, cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), h->stream));
+    }
     CU(h, cudaStreamSynchronize(h->stream));
     h->launch_max_hits = 0;
+    if (gave_up) {
+        // Some lanes stopped part-way: their state no longer matches their walk index.
+        h->initialised = false;
+        h->dump_lanes = 0;
+        h->dump_keys = 0;
+        return fail(h, LXMFV_ERR_CUDA, "a warp-specialised launch gave up waiting on its ring; initialise again");
+    }
     h->dump_lanes = 0;
     h->dump_keys = 0;
     *n_hits = count;
@@ -569,6 +651,7 @@ void lxmfv_close(lxmfv_handle* h) {
         cudaFree(h->d_hits);
         cudaFree(h->d_dump_u);
         cudaFree(h->d_dump_addr);
+        cudaFree(h->d_err);
         if (h->ev0) cudaEventDestroy(h->ev0);
         if (h->ev1) cudaEventDestroy(h->ev1);
         if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);

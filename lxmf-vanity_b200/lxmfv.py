@@ -31,6 +31,7 @@ WALK_GROUP = 0
 WALK_XADD = 1
 FLAG_PHASE_SYNC = 1
 FLAG_REGCAP_80 = 2
+FLAG_WARP_SPEC = 4
 
 # u(8B), the step point of the walk (mod.rs:111): 32 LE bytes.
 U8B = bytes.fromhex("6899c948ed6f71f11ea974adcaed787aa15cb6c84d883bd82d5cd6aad7a65f27")

@@ -39,10 +39,12 @@ class WalkConfig:
     block: int  # threads per block
     sync: bool  # phase barrier
     regcap: int = 128
+    ws: bool = False  # walker and hash warps (LXMFV_FLAG_WARP_SPEC)
 
     @property
     def flags(self) -> int:
         f = lx.FLAG_PHASE_SYNC if self.sync else 0
+        f |= lx.FLAG_WARP_SPEC if self.ws else 0
         return f | (lx.FLAG_REGCAP_80 if self.regcap == 80 else 0)
 
     @property
@@ -59,6 +61,8 @@ def candidates(walks=("group", "xadd"), quick: bool = False) -> list[WalkConfig]
             for block, sync in (shapes if not quick else [(256, True), (512, True)]):
                 out.append(WalkConfig("group", g, block, sync))
         out.append(WalkConfig("group", 256, 256, True, regcap=80))
+        for g in (512, 1024):
+            out.append(WalkConfig("group", g, 512, False, ws=True))
     if "xadd" in walks:
         for b in ((64, 128) if quick else (16, 32, 64, 128)):
             for block, sync in (shapes if not quick else [(512, True)]):
@@ -126,7 +130,7 @@ def tune(device: int = 0, walks=("group", "xadd"), quick: bool = False, keys_per
             results.append({**asdict(cfg), "error": str(e)})
     ok = [r for r in results if "keys_per_s" in r]
     best = max(ok, key=lambda r: r["keys_per_s"])
-    cfg = WalkConfig(best["walk"], best["batch"], best["block"], best["sync"], best["regcap"])
+    cfg = WalkConfig(best["walk"], best["batch"], best["block"], best["sync"], best["regcap"], best["ws"])
     steps = measure_steps(cfg, device, iters_list=(1, 4, 16) if quick else (1, 4, 16, 64, 221))
     best_steps = max(steps, key=lambda r: r["keys_per_s"])
     return {"best": {**best, "iters": best_steps["iters"]}, "configs": results, "steps": steps}

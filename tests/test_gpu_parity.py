@@ -150,6 +150,40 @@ def test_reference_init_interface(backend, lx, oracle):
         assert (keys[t] == walked).all(), t
 
 
+@pytest.mark.parametrize("batch,lanes", [(512, 512), (1024, 300)])
+def test_warp_specialised_walk_matches_oracle(lx, oracle, batch, lanes):
+    """Walker warps hand every key to hash warps through shared memory: the
+    same keys, hashes and hits as the oracle, with a partial last block
+    (300 lanes: 2 blocks of 128 and one of 44), across two launches."""
+    with lx.Backend(device=0, lanes=lanes, batch=batch, flags=lx.FLAG_WARP_SPEC) as b:
+        assert b.batch() == batch and b.threads() == lanes
+        setup = lx.seeded_setup(909 + batch, lanes)
+        b.init_from_scalars(setup.scalars)
+        args = lx.make_launch_args(1, setup.ed_pub, lx.prefix_parse("b0"), max_hits=1 << 14, dump_threads=3,
+                                   dump_keys=batch)
+        hits1, dump1, addr1, n1 = b.launch(args, want_dump=True, want_dump_addr=True)
+        hits2, dump2, _, n2 = b.launch(args, want_dump=True)
+    nh = oracle.name_hash()
+    keys1, keys2 = _keys_of(dump1, 3, batch), _keys_of(dump2, 3, batch)
+    hashes = addr1.reshape(3, batch, 4).astype(">u4").view(np.uint8).reshape(3, batch, 16)
+    for t in range(3):
+        walked = oracle.walk_keys(bytes(setup.scalars[t]), 2 * batch)
+        assert (keys1[t] == walked[:batch]).all() and (keys2[t] == walked[batch:]).all(), t
+        for i in range(0, batch, 7):
+            assert bytes(hashes[t, i]) == oracle.lxmf_address(nh, walked[i].tobytes(), setup.ed_pub)
+    expected = set()
+    for t in range(lanes):
+        h, _ = oracle.search_window(bytes(setup.scalars[t]), setup.ed_pub, nh, oracle.prefix_parse("b0"), 2 * batch)
+        expected.update((t, int(x)) for x in h)
+    assert set(hits1) | set(hits2) == expected and n1 + n2 == len(expected)
+
+
+def test_warp_specialised_walk_refuses_other_shapes(lx):
+    for kw in ({"batch": 256}, {"batch": 1024, "walk": lx.WALK_XADD}, {"batch": 1024, "block": 256}):
+        with pytest.raises(lx.LxmfvError):
+            lx.Backend(device=0, lanes=256, flags=lx.FLAG_WARP_SPEC, **kw)
+
+
 def test_reference_init_interface_at_group_1024(lx, oracle):
     """The largest group (its table in constant memory): Backend::init from
     u(k-8), u(k) gives the oracle's keys, as the ladder start does."""
