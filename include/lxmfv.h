@@ -58,9 +58,9 @@ typedef struct lxmfv_handle lxmfv_handle;
  * per SM, instead of two blocks at up to 128 registers (16 warps).  A point of
  * the autotuner's register-cap sweep. */
 #define LXMFV_FLAG_REGCAP_80 2u
-/* WARP_SPEC (grouped walk, batch 512 or 1024, block 0 or 512): each block's
- * warps split by role.  4 walker warps (32 lanes each, 128 lanes per block)
- * run the field arithmetic and hand every key's u through shared memory to 12
+/* WARP_SPEC (grouped walk, batch 512 or 1024, block 0 or 768): each block's
+ * warps split by role.  8 walker warps (32 lanes each, 256 lanes per block)
+ * run the field arithmetic and hand every key's u through shared memory to 16
  * hash warps, which run the SHA-256 chain and the compare; the two phases of
  * the walk then overlap on the multiply-add and ALU pipes.  The same keys,
  * hashes and hits as the grouped walk.  Its waits are bounded: a launch whose

@@ -120,16 +120,33 @@ const void* xadd_kernel_ptr(uint32_t block, bool sync, bool low_regs, bool dump)
     return dump ? xadd_kernel_ptr_d<B, true>(block, sync, low_regs) : xadd_kernel_ptr_d<B, false>(block, sync, low_regs);
 }
 
-// The warp-specialised grouped walk: 4 walker warps and 12 hash warps per
-// block (512 threads, 128 lanes), 6 slots per walker warp's ring.
-constexpr int kWsF = 4, kWsC = 3, kWsS = 6;
+// The warp-specialised grouped walk: 8 walker warps and 16 hash warps per
+// block (768 threads, 256 lanes), 4 slots per walker warp's ring.  The block
+// is launched at the kernel's register count (80 per thread: 61,440), and the
+// roles then move to 128 registers (walkers: the field arithmetic with the
+// next group's forward product) and 56 (hash warps): 256 x 128 + 512 x 56 =
+// 61,440.  ws_regsplit_fits checks that sum against the built kernel before
+// the first launch.
+constexpr int kWsF = 8, kWsC = 2, kWsS = 4, kWsPRegs = 128, kWsQRegs = 56;
+constexpr uint32_t kWsThreads = 32 * kWsF * (1 + kWsC);
 constexpr uint32_t kWsLanesPerBlock = 32 * kWsF;
 constexpr size_t kWsSmem = sizeof(lxk::WsShared<kWsF, kWsS>);
 
 template <int M>
 const void* ws_kernel_ptr(bool dump) {
-    return dump ? (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, true>
-                : (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, false>;
+    return dump ? (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, true, kWsPRegs, kWsQRegs>
+                : (const void*)lxk::group_walk_ws_kernel<M, kWsF, kWsC, kWsS, false, kWsPRegs, kWsQRegs>;
+}
+
+// Whether the register split fits the registers a block of the built kernel
+// is launched with (setmaxnreg.inc waits for registers the other warps give
+// back; a split above the launch total would wait for ever).
+bool ws_regsplit_fits(const void* fn) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return false;
+    const long have = (long)fa.numRegs * kWsThreads;
+    const long need = 32L * kWsF * kWsPRegs + 32L * kWsF * kWsC * kWsQRegs;
+    return have >= need;
 }
 
 const void* ws_kernel_for(uint32_t batch, bool dump) {
@@ -190,7 +207,7 @@ void launch_group_ws(lxmfv_handle* h, const lxk::EmitArgs& em, uint32_t iters) {
         const unsigned grid = (h->lanes + kWsLanesPerBlock - 1) / kWsLanesPerBlock;
         typedef void (*fn_t)(lxk::WsArgs<M>);
         const fn_t fn = (fn_t)ws_kernel_ptr<M>(em.dump_lanes > 0);
-        fn<<<grid, 32 * kWsF * (1 + kWsC), kWsSmem, h->stream>>>(a);
+        fn<<<grid, kWsThreads, kWsSmem, h->stream>>>(a);
     }
 }
 
@@ -385,9 +402,10 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     h->low_regs = (o.flags & LXMFV_FLAG_REGCAP_80) != 0;
     h->ws = (o.flags & LXMFV_FLAG_WARP_SPEC) != 0;
     if (h->ws && (h->walk != LXMFV_WALK_GROUP || !ws_kernel_for(h->batch, false) || h->low_regs ||
-                  (o.block && o.block != 512)))
-        return fail(h, LXMFV_ERR_ARG, "LXMFV_FLAG_WARP_SPEC needs the grouped walk, batch 512 or 1024 and block 0 or 512");
-    if (h->ws) h->block = 512;
+                  (o.block && o.block != kWsThreads)))
+        return fail(h, LXMFV_ERR_ARG, "LXMFV_FLAG_WARP_SPEC needs the grouped walk, batch 512 or 1024 and block 0 or %u",
+                    kWsThreads);
+    if (h->ws) h->block = kWsThreads;
     if (h->walk != LXMFV_WALK_GROUP && h->walk != LXMFV_WALK_XADD)
         return fail(h, LXMFV_ERR_ARG, "walk %u: 0 grouped, 1 x-only", h->walk);
     if (h->low_regs && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, true))
@@ -425,9 +443,12 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     int per_sm = 0;
     if (h->ws) {
         // The ring buffers take more than the default 48 KB of dynamic shared memory.
-        for (int dump = 0; dump < 2; dump++)
+        for (int dump = 0; dump < 2; dump++) {
+            if (!ws_regsplit_fits(ws_kernel_for(h->batch, dump != 0)))
+                return fail(h, LXMFV_ERR_STATE, "warp-specialised walk: the register split exceeds the launch registers");
             CU(h, cudaFuncSetAttribute(ws_kernel_for(h->batch, dump != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kWsSmem));
+        }
         CU(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ws_kernel_for(h->batch, false), (int)h->block,
                                                             kWsSmem));
         if (per_sm < 1) return fail(h, LXMFV_ERR_CUDA, "warp-specialised walk cannot be resident (batch %u)", h->batch);

@@ -223,8 +223,13 @@ struct WsArgs {
 
 // F walker warps and F * C hash warps per block; F * 32 lanes per block.
 // Threads of walker lanes past the last lane walk a copy of the last lane and
-// neither emit nor store.
-template <int M, int F, int C, int S, bool DUMP>
+// neither emit nor store.  PREGS / QREGS (0: no change): registers per thread
+// the walker and hash warps move to with setmaxnreg after the split.  The
+// split must add up to no more than the block's launch registers (threads x
+// the kernel's register count), else the walkers' increase would wait for
+// registers that never come; the host checks that sum before the first launch
+// (ws_regsplit_fits).  The walker warps must fill whole warpgroups.
+template <int M, int F, int C, int S, bool DUMP, int PREGS = 0, int QREGS = 0>
 static __global__ void __launch_bounds__(32 * F * (1 + C), 1) group_walk_ws_kernel(const __grid_constant__ WsArgs<M> a) {
     extern __shared__ __align__(16) unsigned char ws_smem[];
     WsShared<F, S>& sh = *reinterpret_cast<WsShared<F, S>*>(ws_smem);
@@ -242,6 +247,7 @@ static __global__ void __launch_bounds__(32 * F * (1 + C), 1) group_walk_ws_kern
     const bool active = tid < a.g.lanes;
     const uint32_t lane = active ? tid : a.g.lanes - 1;
     if (warp < F) {
+        if constexpr (PREGS > 0) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(PREGS));
         fe uc = load_fe(a.g.state, 0, lane, a.g.lanes);
         fe vc = load_fe(a.g.state, 1, lane, a.g.lanes);
         uint64_t n = a.g.ns[lane];
@@ -252,6 +258,7 @@ static __global__ void __launch_bounds__(32 * F * (1 + C), 1) group_walk_ws_kern
             a.g.ns[lane] = n;
         }
     } else {
+        if constexpr (QREGS > 0) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(QREGS));
         // Read before this warp's first arrive: the walker warp's final store
         // of ns comes after it has seen that arrive.
         const uint64_t key0 = a.g.ns[lane];

@@ -62,7 +62,7 @@ def candidates(walks=("group", "xadd"), quick: bool = False) -> list[WalkConfig]
                 out.append(WalkConfig("group", g, block, sync))
         out.append(WalkConfig("group", 256, 256, True, regcap=80))
         for g in (512, 1024):
-            out.append(WalkConfig("group", g, 512, False, ws=True))
+            out.append(WalkConfig("group", g, 768, False, ws=True))
     if "xadd" in walks:
         for b in ((64, 128) if quick else (16, 32, 64, 128)):
             for block, sync in (shapes if not quick else [(512, True)]):

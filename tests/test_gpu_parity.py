@@ -150,11 +150,11 @@ def test_reference_init_interface(backend, lx, oracle):
         assert (keys[t] == walked).all(), t
 
 
-@pytest.mark.parametrize("batch,lanes", [(512, 512), (1024, 300)])
+@pytest.mark.parametrize("batch,lanes", [(512, 512), (1024, 600)])
 def test_warp_specialised_walk_matches_oracle(lx, oracle, batch, lanes):
     """Walker warps hand every key to hash warps through shared memory: the
     same keys, hashes and hits as the oracle, with a partial last block
-    (300 lanes: 2 blocks of 128 and one of 44), across two launches."""
+    (600 lanes: 2 blocks of 256 and one of 88), across two launches."""
     with lx.Backend(device=0, lanes=lanes, batch=batch, flags=lx.FLAG_WARP_SPEC) as b:
         assert b.batch() == batch and b.threads() == lanes
         setup = lx.seeded_setup(909 + batch, lanes)
@@ -179,7 +179,7 @@ def test_warp_specialised_walk_matches_oracle(lx, oracle, batch, lanes):
 
 
 def test_warp_specialised_walk_refuses_other_shapes(lx):
-    for kw in ({"batch": 256}, {"batch": 1024, "walk": lx.WALK_XADD}, {"batch": 1024, "block": 256}):
+    for kw in ({"batch": 256}, {"batch": 1024, "walk": lx.WALK_XADD}, {"batch": 1024, "block": 512}):
         with pytest.raises(lx.LxmfvError):
             lx.Backend(device=0, lanes=256, flags=lx.FLAG_WARP_SPEC, **kw)
 
