@@ -411,7 +411,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     if (h->low_regs && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, true))
         return fail(h, LXMFV_ERR_ARG,
                     "LXMFV_FLAG_REGCAP_80 needs the grouped walk, batch 256, block 256 and LXMFV_FLAG_PHASE_SYNC");
-    if (!walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
+    if (!h->ws && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
         return fail(h, LXMFV_ERR_ARG,
                     "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
                     "batch 32, 64, 128, 256, 512, 1024; block 128, 256 or 512)",
