@@ -58,18 +58,21 @@ def field_ops_per_key(walk: str, b: int) -> tuple[float, float]:
     return (5 * m + 13) / b, (2 * m + 255) / b
 
 
-# Per key, from one ncu capture of each kernel (profiles/walk_group_g1024_plain_search.md,
+# Per key, from ncu captures of each kernel on a small case (profiles/walk_group_g1024_plain_search.md,
 # profiles/walk_group_g64_plain_search.md, profiles/walk_xadd_b64_plain_search.md; the G = 512, 256 and x-only
-# B = 128 rows from the earlier captures in profiles/): ALU-pipe lane operations (the binding pipe: ALU pipe
-# active % x 64 lanes x SMs x clock / keys per second), all instructions (smsp__inst_executed x 32 / keys), and
-# DRAM bytes (read + write).
+# B = 128 rows from the earlier captures in profiles/):
+#   alu: ALU-pipe lane operations (the binding pipe): sm__inst_executed_pipe_alu.sum x 32 / keys (earlier rows:
+#        ALU pipe active % x 64 lanes x SMs x clock / keys per second);
+#   imad: IMAD-class instructions per key: sm__inst_executed_pipe_fmaheavy.sum x 32 / keys, the pipe that
+#        executes IMAD, IMAD.HI, IMAD.WIDE and IMAD.X (these kernels run no floating point);
+#   inst: all instructions (smsp__inst_executed.sum x 32 / keys); dram_bytes: DRAM read + write.
 NCU_PER_KEY = {
-    ("group", 1024): {"alu": 3221, "inst": 5764, "dram_bytes": 32.0},
+    ("group", 1024): {"alu": 3213, "imad": 2219, "inst": 5764, "dram_bytes": 32.0},
     ("group", 512): {"alu": 3243, "inst": 5823, "dram_bytes": 31.6},
     ("group", 256): {"alu": 3288, "inst": 5935, "dram_bytes": 31.1},
-    ("group", 64): {"alu": 3556, "inst": 6605, "dram_bytes": 24.8},
+    ("group", 64): {"alu": 3546, "imad": 2678, "inst": 6605, "dram_bytes": 24.8},
     ("xadd", 128): {"alu": 4166, "inst": 8120, "dram_bytes": 131.9},
-    ("xadd", 64): {"alu": 4337, "inst": 8562, "dram_bytes": 132.1},
+    ("xadd", 64): {"alu": 4319, "imad": 3740, "inst": 8562, "dram_bytes": 132.1},
 }
 
 
@@ -533,13 +536,13 @@ def measure(torch, dist, lx, a, dev, rank, world, prefix, walk, batch, total_key
                     "imad": imad_line}
         if "imad" in ncu:
             # The metric's own IMAD fraction: IMAD-class instructions per key
-            # from ncu (every IMAD variant: .HI, .WIDE, .X, .MOV, .SHL) x keys/s
-            # over the measured mad.lo.u32 rate.
+            # from ncu x keys/s over the measured mad.lo.u32 rate.
             imad_ncu = ncu["imad"] * keys_per_s_kernel
             roofline["imad_ncu"] = {"achieved": imad_ncu / 1e12, "peak": imad_peak / 1e12, "unit": "T IMAD/s",
                                     "frac": imad_ncu / imad_peak, "per_key": ncu["imad"],
-                                    "note": "ncu sass__inst_executed_per_opcode, opcode IMAD (all variants), "
-                                            "x 32 lanes / keys; peak = measured mad.lo.u32 rate of this GPU"}
+                                    "note": "IMAD-class instructions per key from ncu (FMA-heavy pipe "
+                                            "instructions x 32 / keys: IMAD, IMAD.HI, IMAD.WIDE, IMAD.X) x keys/s; "
+                                            "peak = measured mad.lo.u32 rate of this GPU (probe)"}
     else:
         roofline = dict(imad_line, bound="imad", traffic=None, alu_peak=alu_peak / 1e12)
     config = {"workload": "plain GPU search (8-hex prefix, lxmf.delivery, seeded walkers, 2^36 keys per run)",
