@@ -141,7 +141,17 @@ def main() -> int:
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--quick", action="store_true", help="a few configurations only")
     p.add_argument("--walk", choices=["group", "xadd", "both"], default="both")
+    p.add_argument("--only", default=None,
+                   help="measure one configuration, WALK:BATCH:BLOCK:SYNC[:ws] (e.g. group:1024:512:1 or "
+                        "group:1024:768:0:ws), and print its line")
+    p.add_argument("--keys-per-launch", type=float, default=2 ** 31)
+    p.add_argument("--launches", type=int, default=3)
     a = p.parse_args()
+    if a.only:
+        f = a.only.split(":")
+        cfg = WalkConfig(f[0], int(f[1]), int(f[2]), f[3] == "1", ws=len(f) > 4 and f[4] == "ws")
+        print(json.dumps(measure(cfg, a.device, keys_per_launch=a.keys_per_launch, launches=a.launches)))
+        return 0
     walks = ("group", "xadd") if a.walk == "both" else (a.walk,)
     r = tune(a.device, walks, a.quick)
     print(json.dumps(r))
