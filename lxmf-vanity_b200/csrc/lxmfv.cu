@@ -73,7 +73,7 @@ int fail(lxmfv_handle* h, int code, const char* fmt, ...) {
                         __FILE__, __LINE__);                                                 \
     } while (0)
 
-constexpr int minb(int block) { return block >= 512 ? 1 : block == 256 ? 2 : 4; }
+constexpr int minb(int block) { return block == 512 ? 1 : block == 256 ? 2 : 4; }
 
 // The kernels for a configuration: block 128 runs without the phase barrier;
 // 256 and 512 with or without it.  `low_regs` (LXMFV_FLAG_REGCAP_80): the
@@ -94,13 +94,6 @@ const void* group_kernel_ptr_d(uint32_t block, bool sync, bool low_regs) {
     if (block == 512)
         return sync ? (const void*)lxk::group_walk_kernel<M, 512, minb(512), true, DUMP>
                     : (const void*)lxk::group_walk_kernel<M, 512, minb(512), false, DUMP>;
-    // 20 and 18 warps per SM: up to 96 registers per thread instead of 128.
-    if (block == 640)
-        return sync ? (const void*)lxk::group_walk_kernel<M, 640, 1, true, DUMP>
-                    : (const void*)lxk::group_walk_kernel<M, 640, 1, false, DUMP>;
-    if (block == 576)
-        return sync ? (const void*)lxk::group_walk_kernel<M, 576, 1, true, DUMP>
-                    : (const void*)lxk::group_walk_kernel<M, 576, 1, false, DUMP>;
     return nullptr;
 }
 
@@ -421,7 +414,7 @@ int lxmfv_open(const lxmfv_options* opts, lxmfv_handle** out) {
     if (!h->ws && !walk_kernel_ptr(h->walk, h->batch, h->block, h->sync, h->low_regs))
         return fail(h, LXMFV_ERR_ARG,
                     "unsupported batch %u / block %u (x-only walk: batch 16, 32, 64, 128; grouped walk: "
-                    "batch 32, 64, 128, 256, 512, 1024; block 128, 256 or 512, grouped walk also 576 or 640)",
+                    "batch 32, 64, 128, 256, 512, 1024; block 128, 256 or 512)",
                     h->batch, h->block);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);

@@ -56,10 +56,9 @@ def candidates(walks=("group", "xadd"), quick: bool = False) -> list[WalkConfig]
     """Every configuration the library builds (a handful with `quick`)."""
     out = []
     shapes = [(128, False), (256, False), (256, True), (512, False), (512, True)]
-    group_shapes = shapes + [(576, True), (640, False), (640, True)]  # 18 and 20 warps per SM at 96 registers
     if "group" in walks:
         for g in ((512, 1024) if quick else (32, 64, 128, 256, 512, 1024)):
-            for block, sync in (group_shapes if not quick else [(512, True), (640, True)]):
+            for block, sync in (shapes if not quick else [(256, True), (512, True)]):
                 out.append(WalkConfig("group", g, block, sync))
         out.append(WalkConfig("group", 256, 256, True, regcap=80))
         for g in (512, 1024):
