@@ -9,7 +9,6 @@ as the timed CPU baseline, never as the thing measured on the GPU.
 from __future__ import annotations
 
 import ctypes as C
-import json
 import os
 import subprocess
 
@@ -29,15 +28,12 @@ _ref = None
 
 
 def ref_dir() -> str:
-    """Where the reference tree is: $LXMFV_REF_DIR, else the reference_path
-    recorded in the repository's BASELINE.json, else '' (not available)."""
+    """Where the reference tree is: $LXMFV_REF_DIR, else a directory named
+    `reference` beside the repository, else '' (not available)."""
     d = os.environ.get("LXMFV_REF_DIR", "")
     if not d:
-        try:
-            with open(os.path.join(os.path.dirname(HERE), "BASELINE.json")) as f:
-                d = json.load(f).get("reference_path", "") or ""
-        except (OSError, ValueError):
-            d = ""
+        beside = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+        d = beside if os.path.isfile(os.path.join(beside, "src", "gpu", "common.h")) else ""
     return d
 
 
