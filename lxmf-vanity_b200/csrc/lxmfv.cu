@@ -573,6 +573,9 @@ int lxmfv_launch_async(lxmfv_handle* h, const lxmfv_launch_args* args) {
     if (!h || !args) return fail(h, LXMFV_ERR_ARG, "null argument");
     if (!h->initialised) return fail(h, LXMFV_ERR_STATE, "launch before init");
     if (args->iters == 0) return fail(h, LXMFV_ERR_ARG, "iters must be at least 1");
+    // The warp-specialised walk counts its ring's hand-overs (iters x (M + 1)) in 32 bits.
+    if (h->ws && (uint64_t)args->iters * (h->batch / 2 + 1) >= (1ull << 32))
+        return fail(h, LXMFV_ERR_ARG, "iters %u too large for the warp-specialised walk", args->iters);
     if (int rc = set_device(h)) return rc;
     // The step point is fixed: both walks' tables and start points are built
     // from u(8B), so a launch must use it too (the reference passes it per
