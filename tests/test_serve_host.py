@@ -106,3 +106,21 @@ def test_a_request_larger_than_the_pool_fails_at_once():
     out = srv.serve(pool, reqs, time_limit=60)
     assert reqs[1].failed and out["failed"] == 1 and out["done"] == 2
     assert out["rechecked_bad"] == 0
+
+
+def test_wall_clock_time_to_hit_is_normalised_by_the_requests_own_rate():
+    """wall_time_to_hit: (done - arrival) over 16^L at the request's rate in
+    the pool (keys walked over done - admitted); the queue wait raises it, a
+    slower pool does not."""
+    spec = srv.SearchSpec.seeded(5, "abcde", lanes=32)  # 5 nibbles: 16^5 expected tries
+    expected = 16.0 ** 5
+    fast = srv.Request(arrival=0.0, spec=spec, admitted=0.0, done=1.0, walked=int(expected), tries=int(expected))
+    slow = srv.Request(arrival=0.0, spec=spec, admitted=0.0, done=2.0, walked=int(expected), tries=int(expected))
+    waited = srv.Request(arrival=0.0, spec=spec, admitted=1.0, done=2.0, walked=int(expected), tries=int(expected))
+    assert srv.wall_time_to_hit(fast) == pytest.approx(1.0)
+    assert srv.wall_time_to_hit(slow) == pytest.approx(1.0)   # the same keys at half the rate
+    assert srv.wall_time_to_hit(waited) == pytest.approx(2.0)  # a second of queue wait before a second in the pool
+    out = srv.summarise([fast, slow, waited], [fast, slow, waited], wall=2.0, keys=3 * int(expected), busy_ms=2000.0,
+                        steps=3, bad=0, lane_rate=expected / 32)
+    assert out["time_to_hit_over_expected"]["p50"] == pytest.approx(1.0)
+    assert out["time_to_hit_at_pool_rate"]["p50"] == pytest.approx(2.0)  # 2 s at the pool's mean rate of 1 per s
