@@ -61,3 +61,19 @@ def test_a_world_size_other_than_gpus_is_refused():
     p = _bench(["--gpus", "2", "--steps", "1", "--warmup", "3", "--engine", "tests.bench_stub:measure"],
                _env(WORLD_SIZE="1", RANK="0", LOCAL_RANK="0"))
     assert p.returncode != 0 and "does not match" in p.stderr
+
+
+def test_every_default_section_has_its_ncu_counts():
+    """The bench's roofline for each default plain-search section (the headline
+    G, and B = 64 for both walks) comes from per-key ncu counts: ALU-pipe and
+    IMAD-class instructions, all instructions and DRAM bytes."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    for key in (("group", bench.BATCH), ("group", 64), ("xadd", 64)):
+        counts = bench.NCU_PER_KEY[key]
+        assert {"alu", "imad", "inst", "dram_bytes"} <= set(counts), key
+        assert counts["alu"] + counts["imad"] < counts["inst"]
+    # The algorithmic field work per key falls as the group grows (one inversion per G keys).
+    assert bench.wide_products_per_key("group", 1024) < bench.wide_products_per_key("group", 64)
+    assert bench.wide_products_per_key("group", 64) < bench.wide_products_per_key("xadd", 64)
