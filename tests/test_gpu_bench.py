@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_bench_line_on_a_small_search():
-    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--lanes", "4096", "--total-keys", "2e8",
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--total-keys", "2e9",
                         "--steps", "2", "--warmup", "3", "--no-cpu-baseline", "--no-cpu-search", "--no-ref-cuda",
                         "--no-batched", "--served-seconds", "0"], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
