@@ -380,8 +380,8 @@ int lxmfv_fe_op(lxmfv_handle* h, int op, const uint32_t* a, const uint32_t* b, u
  * count above LXMFV_STATIC_SCRATCH_ELEMS is rejected with LXMFV_ERR_ARG, and
  * calls whose kernels overlap on the GPU race on the array, so the caller
  * must order them.  The first call in a device's context looks up the
- * array's device address with that device current; make it before any
- * stream capture.  After cudaDeviceReset the next call looks it up again.
+ * array's device address with that device current.  After cudaDeviceReset
+ * the next call looks it up again.
  * A message for a non-zero return goes to err (err_len bytes) when given. */
 int lxmfv_fe_batch_invert_static(const uint32_t* d_a, uint32_t* d_out, uint64_t count, uint32_t group, void* stream,
                                  char* err, size_t err_len);

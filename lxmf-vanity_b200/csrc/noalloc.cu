@@ -22,9 +22,9 @@
 //   - count <= LXMFV_STATIC_SCRATCH_ELEMS, else LXMFV_ERR_ARG and nothing runs;
 //   - the first call in a CUDA context (the device's primary context, made
 //     current by the runtime) looks up the scratch array's device address
-//     with cudaGetSymbolAddress; make that first call before any stream
-//     capture.  After cudaDeviceReset the runtime gives the device a new
-//     context, and the next call looks the address up again;
+//     with cudaGetSymbolAddress.  After cudaDeviceReset the runtime gives
+//     the device a new context, and the next call looks the address up
+//     again;
 //   - every call shares the one array: calls whose kernels overlap on the
 //     GPU (two streams, or two host threads) race on it and must be ordered
 //     by the caller.  Nothing in the array needs to start at zero: each
