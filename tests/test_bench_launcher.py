@@ -77,3 +77,17 @@ def test_every_default_section_has_its_ncu_counts():
     # The algorithmic field work per key falls as the group grows (one inversion per G keys).
     assert bench.wide_products_per_key("group", 1024) < bench.wide_products_per_key("group", 64)
     assert bench.wide_products_per_key("group", 64) < bench.wide_products_per_key("xadd", 64)
+
+
+def test_reference_arm_under_two_ranks_prints_one_line():
+    """`bench.py --impl reference --gpus 2`, as the scaling run launches it:
+    rank 0 alone times the reference's CPU walk and prints one line with
+    impl "reference"; the other rank exits 0 without work."""
+    p = _bench(["--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3"], _env())
+    assert p.returncode == 0, p.stderr[-3000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, p.stdout
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
